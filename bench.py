@@ -1,0 +1,447 @@
+"""bench.py -- output GB/s of the rocRAND host-API generation path on B200.
+
+Workload (one "step"): the plain single-generator sweep at n = 2^28 values per call --
+every generator family built so far x {raw uint32, uniform fp32/fp64/fp16, normal fp32/fp64,
+log-normal fp32, Poisson lambda in {0.5, 10, 1000}} at seed 0xdeadbeef -- each call one
+rocrand_generate_* through the C ABI into a resident device buffer.  Outputs (0.5-2 GiB per
+call) are larger than L2, so no flush is needed between calls.
+
+value  = total output bytes / device time of the K timed steps (CUDA events, max over ranks);
+e2e    = the same sweep through the same C ABI with the output copied to pinned host memory
+         inside the timed region (what a host caller gets);
+roofline = the dominant kernel's achieved write GB/s against the measured HBM copy peak;
+cpu_baseline = the reference's own host generators (oracle/_ref, compiled from the reference
+         sources) on this host's cores, on a bounded sample of the same sweep.
+
+--impl reference runs only the reference's CPU host generators on the same workload.
+Multi-GPU (torchrun): each rank fills its own disjoint slice of every stream (offset =
+rank * n), no data-path collective; weak scaling.
+"""
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from ctypes import c_size_t, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+SEED = 0xDEADBEEF
+FALLBACK_HBM_GBS = 6650.0
+
+# Generator families in the sweep (rocrand_rng_type values), in the order they were built.
+SWEEP_GENERATORS = [("philox4x32_10", 404)]
+SWEEP_DISTS = [
+    ("uint", None), ("uniform", None), ("uniform_double", None), ("uniform_half", None),
+    ("normal", (0.0, 1.0)), ("normal_double", (0.0, 1.0)), ("log_normal", (0.0, 1.0)),
+    ("poisson", (0.5,)), ("poisson", (10.0,)), ("poisson", (1000.0,)),
+]
+ELEM = {"uint": 4, "uniform": 4, "uniform_double": 8, "uniform_half": 2, "normal": 4,
+        "normal_double": 8, "log_normal": 4, "poisson": 4, "char": 1, "short": 2}
+ENTRY = {"uint": "rocrand_generate", "uniform": "rocrand_generate_uniform",
+         "uniform_double": "rocrand_generate_uniform_double",
+         "uniform_half": "rocrand_generate_uniform_half", "normal": "rocrand_generate_normal",
+         "normal_double": "rocrand_generate_normal_double",
+         "log_normal": "rocrand_generate_log_normal", "poisson": "rocrand_generate_poisson"}
+
+
+def call_args(dist, params):
+    if params is None:
+        return []
+    if dist in ("normal", "log_normal"):
+        return [ctypes.c_float(params[0]), ctypes.c_float(params[1])]
+    if dist in ("normal_double", "log_normal_double"):
+        return [ctypes.c_double(params[0]), ctypes.c_double(params[1])]
+    return [ctypes.c_double(params[0])]
+
+
+def stream_offset(dist, first_value):
+    """Engine offset that starts a stream slice at output `first_value` (aligned outputs):
+    inputs per output = iw/ow of the distribution."""
+    per = {"uniform_double": 2.0, "normal_double": 2.0, "log_normal_double": 2.0,
+           "uniform_half": 0.5, "char": 0.25, "short": 0.5}.get(dist, 1.0)
+    return int(first_value * per)
+
+
+def measured_peak():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            # nvidia-smi takes a moment to print its first sample: wait for it so the
+            # timed region is covered from its start.
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0:
+                time.sleep(0.02)
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def select_calls(only):
+    """The sweep's calls, optionally filtered by "gen:dist[:param],..." (e.g. the single
+    kernel an ncu capture looks at)."""
+    calls = [(gname, gtype, d, p) for gname, gtype in SWEEP_GENERATORS for d, p in SWEEP_DISTS]
+    if not only:
+        return calls
+    keep = []
+    for item in only.split(","):
+        parts = item.split(":")
+        for c in calls:
+            if c[0] == parts[0] and c[2] == parts[1] and (
+                    len(parts) < 3 or (c[3] is not None and float(parts[2]) == c[3][0])):
+                keep.append(c)
+    if not keep:
+        raise SystemExit("--only matched no call: %s" % only)
+    return keep
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ------------------------------------------------------------------------------------
+# our arm
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import rocrand_b200 as rb
+    lib = rb.load_library()
+
+    n = args.n
+    calls = select_calls(args.only)
+    max_bytes = max(ELEM[d] for _, _, d, _ in calls) * n
+    out = torch.empty(max_bytes, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    gens = {}
+    for gname, gtype, d, p in calls:
+        g = c_void_p()
+        rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), gtype))
+        rb.check_rocrand(lib.rocrand_set_seed(g, SEED))
+        rb.check_rocrand(lib.rocrand_set_offset(g, stream_offset(d, rank * n)))
+        rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
+        gens[(gname, d, p)] = g
+
+    def one_call(c, ptr):
+        gname, gtype, d, p = c
+        st = getattr(lib, ENTRY[d])(gens[(gname, d, p)], c_void_p(ptr), c_size_t(n), *call_args(d, p))
+        if st != 0:
+            raise rb.RocRandError(st)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        for c in calls:
+            one_call(c, out.data_ptr())
+    barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(len(calls) + 1)] for _ in range(args.steps)]
+    barrier()
+    for s in range(args.steps):
+        evs[s][0].record(stream)
+        for i, c in enumerate(calls):
+            one_call(c, out.data_ptr())
+            evs[s][i + 1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [evs[s][0].elapsed_time(evs[s][-1]) for s in range(args.steps)]
+    per_call_ms = [[evs[s][i].elapsed_time(evs[s][i + 1]) for i in range(len(calls))] for s in range(args.steps)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    step_bytes = sum(ELEM[d] * n for _, _, d, _ in calls)
+    value = step_bytes * world * args.steps / (total_ms * 1e-3) / 1e9
+
+    # dominant kernel: the call with the largest device time in the step
+    mean_call = [statistics.mean(per_call_ms[s][i] for s in range(args.steps)) for i in range(len(calls))]
+    dom = max(range(len(calls)), key=lambda i: mean_call[i])
+    peak, peak_kind = measured_peak()
+    dom_bytes = ELEM[calls[dom][2]] * n
+    dom_gbs = dom_bytes / (mean_call[dom] * 1e-3) / 1e9
+    # north-star kernel: Philox uniform fp32 at 2^28
+    ns = [i for i, c in enumerate(calls) if c[0] == "philox4x32_10" and c[2] == "uniform"]
+    ns_gbs = (4 * n) / (mean_call[ns[0]] * 1e-3) / 1e9 if ns else None
+
+    # e2e through the same C ABI with pinned host output, copies inside the timed region
+    host = torch.empty(max_bytes, dtype=torch.uint8, pin_memory=True)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    d2h = 0
+    for _ in range(e2e_steps):
+        for c in calls:
+            one_call(c, out.data_ptr())
+            nb = ELEM[c[2]] * n
+            host[:nb].copy_(out[:nb], non_blocking=True)
+            d2h += nb
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = step_bytes * world * e2e_steps / (e2e_ms * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args.cpu_n, calls)
+
+    for g in gens.values():
+        lib.rocrand_destroy_generator(g)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+    if rank != 0:
+        return
+    line = {
+        "metric": "output GB/s of rocrand_generate_* (bit-exact vs reference host generators)",
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32/f32/f64/f16 outputs, int32 engine arithmetic",
+        "data": "synthetic: seeded generator streams (seed 0xdeadbeef), no input data",
+        "config": {
+            "workload": "plain single-generator sweep, n=2^28 values per call",
+            "generators": [g for g, _ in SWEEP_GENERATORS],
+            "distributions": ["%s%s" % (d, "" if p is None else str(list(p))) for d, p in SWEEP_DISTS],
+            "n_per_call": n,
+            "bytes_per_step_per_gpu": step_bytes,
+            "l2": "outputs 0.5-2 GiB per call > 126 MB L2; no flush needed",
+            "parallelism": "replica shards: rank r fills stream slice [r*n, (r+1)*n)",
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "%s %s" % (calls[dom][0], calls[dom][2]),
+            "achieved": round(dom_gbs, 1),
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(dom_gbs / peak, 4),
+            "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs copy bandwidth)" % peak_kind
+            if peak_kind == "measured" else "fallback 6650 GB/s",
+            "traffic": None,
+            "algorithmic_bytes_per_launch": dom_bytes,
+        },
+        "north_star": {"kernel": "philox4x32_10 uniform fp32 n=2^28",
+                       "achieved_gbs": round(ns_gbs, 1) if ns_gbs else None,
+                       "frac_of_peak": round(ns_gbs / peak, 4) if ns_gbs else None},
+        "per_call_ms": {"%s %s%s" % (c[0], c[2], "" if c[3] is None else list(c[3])): round(mean_call[i], 4)
+                        for i, c in enumerate(calls)},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": step_bytes,
+                "how": "same C-ABI calls + D2H copy of every output to pinned host memory, %d steps" % e2e_steps},
+        "gpu_launches": len(calls) * args.steps,
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------------------
+# reference host generators (CPU)
+
+
+def _ref_lib():
+    from oracle import pyorc
+    if os.path.exists(pyorc.REF_PATH):
+        return pyorc.CLib("ref"), "reference"
+    return pyorc.CLib("orc"), "port"
+
+
+def cpu_sample(n_per_call, calls, threads):
+    """Runs every call of the sweep on the reference's host generators, n_per_call values
+    each, split over `threads` host threads (each its own generator, offset to its slice).
+    Returns (bytes, seconds, kind)."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import pyorc
+    lib, kind = _ref_lib()
+    total_bytes = 0
+    t_all = 0.0
+    for gname, gtype, d, p in calls:
+        suffix, dt, _ = pyorc.DISTS[d]
+        buf = np.empty(n_per_call + 64, dtype=dt)
+        base = (-buf.ctypes.data // buf.itemsize) % (64 // buf.itemsize)
+        view = buf[base:base + n_per_call]
+        chunk = (n_per_call // threads) // 64 * 64
+        bounds = [(i * chunk, (i + 1) * chunk if i < threads - 1 else n_per_call) for i in range(threads)]
+        gens = []
+        for a, b in bounds:
+            g = lib.create(gtype)
+            lib.set_seed(g, SEED)
+            lib.set_offset(g, stream_offset(d, a))
+            gens.append(g)
+        fn = lib.fn(suffix)
+        args = pyorc.dist_args(d, p if p is not None else ())
+
+        def work(i):
+            a, b = bounds[i]
+            return fn(gens[i], c_void_p(view[a:b].ctypes.data), c_size_t(b - a), *args)
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            sts = list(ex.map(work, range(threads)))
+        t_all += time.perf_counter() - t0
+        assert all(s == 0 for s in sts), sts
+        for g in gens:
+            lib.destroy(g)
+        total_bytes += n_per_call * buf.itemsize
+    return total_bytes, t_all, kind
+
+
+def cpu_baseline_sample(n_per_call, calls):
+    threads = os.cpu_count() or 1
+    nb, secs, kind = cpu_sample(n_per_call, calls, threads)
+    return {"value": round(nb / secs / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": "same sweep at n=%d values per call (vs 2^28 on the GPU), %d host threads, "
+                      "each its own host generator on a disjoint offset slice" % (n_per_call, threads)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    calls = select_calls(args.only)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(args.cpu_n // 4, calls, threads)
+    nb = 0
+    secs = 0.0
+    kind = None
+    for _ in range(args.steps):
+        b, s, kind = cpu_sample(args.cpu_n, calls, threads)
+        nb += b
+        secs += s
+    value = nb / secs / 1e9
+    line = {
+        "impl": "reference",
+        "metric": "output GB/s of rocrand_generate_* (bit-exact vs reference host generators)",
+        "value": round(value, 3),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(secs / args.steps * 1e3, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32/f32/f64/f16 outputs, int32 engine arithmetic",
+        "data": "synthetic: seeded generator streams (seed 0xdeadbeef), no input data",
+        "config": {"workload": "plain single-generator sweep, n=2^28 values per call (sampled)",
+                   "generators": [g for g, _ in SWEEP_GENERATORS], "n_per_call_sampled": args.cpu_n},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+                         "sample": "n=%d values per call per step, %d threads" % (args.cpu_n, threads)},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 28)
+    ap.add_argument("--cpu-n", type=int, default=1 << 24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default="", help="gen:dist[:param],... subset of the sweep")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,298 @@
+// api.cpp -- the extern "C" rocRAND host ABI of librocrand (B200 build).
+//
+// Same entry points, argument meaning and status codes as the reference's
+// library/src/rocrand.cpp:111-634: a NULL generator gives NOT_CREATED, lambda <= 0 gives
+// OUT_OF_RANGE, unknown generator types give TYPE_ERROR, and no C++ exception crosses the
+// ABI (rocrand.cpp:92-99).
+#include "common.hpp"
+#include "generators.hpp"
+
+#include <cuda_fp16.h>
+
+#include <new>
+
+namespace rb200
+{
+
+const DeviceInfo& device_info()
+{
+    // One entry per device, filled on first use on that device.
+    static thread_local DeviceInfo cache[64];
+    static thread_local bool       valid[64] = {};
+    int                            dev       = 0;
+    cudaGetDevice(&dev);
+    if(dev < 0 || dev >= 64)
+        dev = 0;
+    if(!valid[dev])
+    {
+        int sms = 0;
+        if(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess
+           || sms <= 0)
+            sms = 148;
+        cache[dev].device   = dev;
+        cache[dev].sm_count = sms;
+        valid[dev]          = true;
+    }
+    return cache[dev];
+}
+
+static rocrand_generator_base_type* make_generator(rocrand_rng_type t)
+{
+    switch(t)
+    {
+        case ROCRAND_RNG_PSEUDO_PHILOX4_32_10: return new PhiloxGenerator();
+        default: return nullptr;
+    }
+}
+
+template<class Fn>
+static rocrand_status guarded(Fn&& fn)
+{
+    try
+    {
+        return fn();
+    }
+    catch(const std::bad_alloc&)
+    {
+        return ROCRAND_STATUS_ALLOCATION_FAILED;
+    }
+    catch(rocrand_status s)
+    {
+        return s;
+    }
+    catch(...)
+    {
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+}
+
+static uint16_t half_bits(half h)
+{
+    return __half_as_ushort(h);
+}
+
+} // namespace rb200
+
+using namespace rb200;
+
+extern "C" {
+
+rocrand_status ROCRANDAPI rocrand_create_generator(rocrand_generator* generator,
+                                                   rocrand_rng_type   rng_type)
+{
+    if(generator == nullptr)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    return guarded([&] {
+        rocrand_generator_base_type* g = make_generator(rng_type);
+        if(g == nullptr)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        *generator = g;
+        return ROCRAND_STATUS_SUCCESS;
+    });
+}
+
+rocrand_status ROCRANDAPI rocrand_create_generator_host(rocrand_generator* generator,
+                                                        rocrand_rng_type   rng_type)
+{
+    (void)generator;
+    (void)rng_type;
+    return ROCRAND_STATUS_TYPE_ERROR;
+}
+
+rocrand_status ROCRANDAPI rocrand_create_generator_host_blocking(rocrand_generator* generator,
+                                                                 rocrand_rng_type   rng_type)
+{
+    (void)generator;
+    (void)rng_type;
+    return ROCRAND_STATUS_TYPE_ERROR;
+}
+
+rocrand_status ROCRANDAPI rocrand_destroy_generator(rocrand_generator generator)
+{
+    return guarded([&] {
+        delete generator;
+        return ROCRAND_STATUS_SUCCESS;
+    });
+}
+
+#define RB200_GEN(generator, body)                   \
+    do                                               \
+    {                                                \
+        if((generator) == nullptr)                   \
+            return ROCRAND_STATUS_NOT_CREATED;       \
+        return guarded([&] { return (body); });      \
+    }                                                \
+    while(0)
+
+rocrand_status ROCRANDAPI rocrand_generate(rocrand_generator generator,
+                                           unsigned int*     output_data,
+                                           size_t            n)
+{
+    RB200_GEN(generator, generator->generate(output_data, n, Dist::U32, DistParams{}));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_long_long(rocrand_generator       generator,
+                                                     unsigned long long int* output_data,
+                                                     size_t                  n)
+{
+    RB200_GEN(generator, generator->generate(output_data, n, Dist::U64, DistParams{}));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_char(rocrand_generator generator,
+                                                unsigned char*    output_data,
+                                                size_t            n)
+{
+    RB200_GEN(generator, generator->generate(output_data, n, Dist::U8, DistParams{}));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_short(rocrand_generator generator,
+                                                 unsigned short*   output_data,
+                                                 size_t            n)
+{
+    RB200_GEN(generator, generator->generate(output_data, n, Dist::U16, DistParams{}));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_uniform(rocrand_generator generator,
+                                                   float*            output_data,
+                                                   size_t            n)
+{
+    RB200_GEN(generator, generator->generate(output_data, n, Dist::F32, DistParams{}));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_uniform_double(rocrand_generator generator,
+                                                          double*           output_data,
+                                                          size_t            n)
+{
+    RB200_GEN(generator, generator->generate(output_data, n, Dist::F64, DistParams{}));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_uniform_half(rocrand_generator generator,
+                                                        half*             output_data,
+                                                        size_t            n)
+{
+    RB200_GEN(generator, generator->generate(output_data, n, Dist::F16, DistParams{}));
+}
+
+static DistParams params_f(float mean, float stddev)
+{
+    DistParams p;
+    p.mean_f = mean;
+    p.std_f  = stddev;
+    return p;
+}
+
+static DistParams params_d(double mean, double stddev)
+{
+    DistParams p;
+    p.mean_d = mean;
+    p.std_d  = stddev;
+    return p;
+}
+
+static DistParams params_h(half mean, half stddev)
+{
+    DistParams p;
+    p.mean_h = half_bits(mean);
+    p.std_h  = half_bits(stddev);
+    return p;
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_normal(
+    rocrand_generator generator, float* output_data, size_t n, float mean, float stddev)
+{
+    RB200_GEN(generator,
+              generator->generate(output_data, n, Dist::NORMAL_F32, params_f(mean, stddev)));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_normal_double(
+    rocrand_generator generator, double* output_data, size_t n, double mean, double stddev)
+{
+    RB200_GEN(generator,
+              generator->generate(output_data, n, Dist::NORMAL_F64, params_d(mean, stddev)));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_normal_half(
+    rocrand_generator generator, half* output_data, size_t n, half mean, half stddev)
+{
+    RB200_GEN(generator,
+              generator->generate(output_data, n, Dist::NORMAL_F16, params_h(mean, stddev)));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_log_normal(
+    rocrand_generator generator, float* output_data, size_t n, float mean, float stddev)
+{
+    RB200_GEN(generator,
+              generator->generate(output_data, n, Dist::LOGNORMAL_F32, params_f(mean, stddev)));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_log_normal_double(
+    rocrand_generator generator, double* output_data, size_t n, double mean, double stddev)
+{
+    RB200_GEN(generator,
+              generator->generate(output_data, n, Dist::LOGNORMAL_F64, params_d(mean, stddev)));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_log_normal_half(
+    rocrand_generator generator, half* output_data, size_t n, half mean, half stddev)
+{
+    RB200_GEN(generator,
+              generator->generate(output_data, n, Dist::LOGNORMAL_F16, params_h(mean, stddev)));
+}
+
+rocrand_status ROCRANDAPI rocrand_generate_poisson(rocrand_generator generator,
+                                                   unsigned int*     output_data,
+                                                   size_t            n,
+                                                   double            lambda)
+{
+    if(generator == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    if(lambda <= 0.0)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    return guarded([&] { return generator->generate_poisson(output_data, n, lambda); });
+}
+
+rocrand_status ROCRANDAPI rocrand_initialize_generator(rocrand_generator generator)
+{
+    RB200_GEN(generator, generator->init());
+}
+
+rocrand_status ROCRANDAPI rocrand_set_stream(rocrand_generator generator, hipStream_t stream)
+{
+    RB200_GEN(generator, generator->set_stream(stream));
+}
+
+rocrand_status ROCRANDAPI rocrand_set_seed(rocrand_generator generator, unsigned long long seed)
+{
+    RB200_GEN(generator, generator->set_seed(seed));
+}
+
+rocrand_status ROCRANDAPI rocrand_set_seed_uint4(rocrand_generator generator, uint4 seed)
+{
+    RB200_GEN(generator, generator->set_seed_uint4(seed));
+}
+
+rocrand_status ROCRANDAPI rocrand_set_offset(rocrand_generator generator, unsigned long long offset)
+{
+    RB200_GEN(generator, generator->set_offset(offset));
+}
+
+rocrand_status ROCRANDAPI rocrand_set_ordering(rocrand_generator generator, rocrand_ordering order)
+{
+    RB200_GEN(generator, generator->set_order(order));
+}
+
+rocrand_status ROCRANDAPI rocrand_set_quasi_random_generator_dimensions(rocrand_generator generator,
+                                                                        unsigned int dimensions)
+{
+    RB200_GEN(generator, generator->set_dimensions(dimensions));
+}
+
+rocrand_status ROCRANDAPI rocrand_get_version(int* version)
+{
+    if(version == nullptr)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    *version = ROCRAND_VERSION;
+    return ROCRAND_STATUS_SUCCESS;
+}
+
+} // extern "C"

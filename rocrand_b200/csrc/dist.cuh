@@ -1,0 +1,389 @@
+// dist.cuh -- distribution functors fused into the generator kernels (sm_100a).
+//
+// Each functor reproduces one host functor of the reference (library/src/rng/distribution/
+// *.hpp) together with the scalar conversion it calls in the *host* branch of
+// library/include/rocrand/rocrand_{uniform,normal,discrete}.h, because parity is judged
+// against the reference's host generators.  Every rounding step is written with an
+// explicit _rn intrinsic: a product is fused into an FMA only where it is exact (scaling
+// by a power of two), so the device rounds exactly where the x86-64 host does.
+// Transcendentals (log/sin/cos/exp) use CUDA's accurate library functions; they can
+// differ from glibc by an ulp or two, which is the stated tolerance for normal and
+// log-normal outputs.
+#pragma once
+
+#include "common.hpp"
+
+#include <cuda_fp16.h>
+
+#include <cstdint>
+
+namespace rb200
+{
+
+// Constants of rocrand_common.h:24-36, spelled as the reference spells them so that they
+// round to the same binary values.
+#define RB_2POW16_INV (1.5258789e-05f)
+#define RB_2POW16_INV_2PI (9.58738e-05f)
+#define RB_2POW32_INV (2.3283064e-10f)
+#define RB_2POW32_INV_DOUBLE (2.3283064365386963e-10)
+#define RB_2POW32_INV_2PI (1.46291807e-09f)
+#define RB_2POW53_INV_DOUBLE (1.1102230246251565e-16)
+#define RB_PI_DOUBLE (3.1415926535897932)
+#define RB_SQRT2 (1.4142135f)
+
+// ---- scalar conversions ----
+
+// rocrand_uniform.h:61-64: 2^-32 + v * 2^-32 (exact product, one rounding).
+__device__ __forceinline__ float u32_to_f32(uint32_t v)
+{
+    return __fmaf_rn(__uint2float_rn(v), RB_2POW32_INV, RB_2POW32_INV);
+}
+
+// rocrand_uniform.h:97-107: 53 bits from (v1, v2 >> 11), 2^-53 + v * 2^-53.
+__device__ __forceinline__ double u32x2_to_f64(uint32_t v1, uint32_t v2)
+{
+    const uint64_t v = (uint64_t)v1 | ((uint64_t)(v2 >> 11) << 32);
+    return __fma_rn(__ull2double_rn(v), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+}
+
+// rocrand_uniform.h:92-95: 2^-32 + v * 2^-32 in double (exact).
+__device__ __forceinline__ double u32_to_f64(uint32_t v)
+{
+    return __fma_rn(__uint2double_rn(v), RB_2POW32_INV_DOUBLE, RB_2POW32_INV_DOUBLE);
+}
+
+// rocrand_uniform.h:150-153: half of 2^-16 + v * 2^-16 (float math exact, RNE to half).
+__device__ __forceinline__ __half u16_to_f16(uint32_t v16)
+{
+    return __float2half_rn(__fmaf_rn((float)(v16 & 0xffffu), RB_2POW16_INV, RB_2POW16_INV));
+}
+
+// rocrand_normal.h:51-66 (host branch: sinf/cosf on the rounded angle).
+__device__ __forceinline__ float2 box_muller_f32(uint32_t x, uint32_t y)
+{
+    const float u = __fmaf_rn(__uint2float_rn(x), RB_2POW32_INV, RB_2POW32_INV);
+    const float v = __fadd_rn(RB_2POW32_INV_2PI, __fmul_rn(__uint2float_rn(y), RB_2POW32_INV_2PI));
+    const float s = __fsqrt_rn(__fmul_rn(-2.0f, logf(u)));
+    float       sv, cv;
+    sincosf(v, &sv, &cv);
+    return make_float2(__fmul_rn(sv, s), __fmul_rn(cv, s));
+}
+
+// rocrand_normal.h:68-89 (host branch: sin/cos of w * pi rounded in double).
+__device__ __forceinline__ double2 box_muller_f64(uint32_t x, uint32_t y, uint32_t z, uint32_t w)
+{
+    const uint64_t v1 = (uint64_t)x ^ ((uint64_t)y << 21);
+    const double   u  = __fma_rn(__ull2double_rn(v1), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+    const uint64_t v2 = (uint64_t)z ^ ((uint64_t)w << 21);
+    const double   ww = __fma_rn(__ull2double_rn(v2), RB_2POW53_INV_DOUBLE * 2.0, RB_2POW53_INV_DOUBLE * 2.0);
+    const double   s  = __dsqrt_rn(__dmul_rn(-2.0, log(u)));
+    const double   a  = __dmul_rn(ww, RB_PI_DOUBLE);
+    double         sv, cv;
+    sincos(a, &sv, &cv);
+    return make_double2(__dmul_rn(sv, s), __dmul_rn(cv, s));
+}
+
+// rocrand_normal.h:102-122, float branch used by the host build; halves of the results.
+__device__ __forceinline__ void box_muller_f16(uint32_t v, __half r[2])
+{
+    const float u = __fmaf_rn((float)(v & 0xffffu), RB_2POW16_INV, RB_2POW16_INV);
+    const float a = __fadd_rn(RB_2POW16_INV_2PI, __fmul_rn((float)(v >> 16), RB_2POW16_INV_2PI));
+    const float s = __fsqrt_rn(__fmul_rn(-2.0f, logf(u)));
+    float       sv, cv;
+    sincosf(a, &sv, &cv);
+    r[0] = __float2half_rn(__fmul_rn(sv, s));
+    r[1] = __float2half_rn(__fmul_rn(cv, s));
+}
+
+// rocrand_normal.h:196-220 roc_d_erfinv (host branch).
+__device__ __forceinline__ double erfinv_d(double x)
+{
+    const double sgn = (x < 0.0) ? -1.0 : 1.0;
+    x                = __dmul_rn(__dsub_rn(1.0, x), __dadd_rn(1.0, x));
+    const double lnx = log(x);
+    if(isnan(lnx))
+        return 1.0;
+    if(isinf(lnx))
+        return 0.0;
+    const double tt1 = __dadd_rn(2.0 / (RB_PI_DOUBLE * 0.147), __dmul_rn(0.5, lnx));
+    const double tt2 = __dmul_rn(1.0 / (0.147), lnx);
+    return sgn * __dsqrt_rn(__dadd_rn(-tt1, __dsqrt_rn(__dsub_rn(__dmul_rn(tt1, tt1), tt2))));
+}
+
+// rocrand_normal.h:265-270: sqrt(2) is a float literal promoted to double.
+__device__ __forceinline__ double normal_from_u32_f64(uint32_t x)
+{
+    const double p = u32_to_f64(x);
+    return __dmul_rn((double)RB_SQRT2, erfinv_d(__dsub_rn(__dmul_rn(2.0, p), 1.0)));
+}
+
+// rocrand_discrete.h:33-60 discrete_alias for a 32-bit input.
+__device__ __forceinline__ uint32_t alias_lookup(uint32_t r, uint32_t size, uint32_t offset,
+                                                 const double* prob, const uint32_t* alias)
+{
+    const double   x   = __dmul_rn(__uint2double_rn(r), RB_2POW32_INV_DOUBLE);
+    const double   nx  = __dmul_rn(__uint2double_rn(size), x);
+    const double   fnx = floor(nx);
+    const double   y   = __dsub_rn(nx, fnx);
+    const uint32_t i   = __double2uint_rz(fnx);
+    return offset + (y < prob[i] ? i : alias[i]);
+}
+
+// poisson.hpp:80-108 poisson_distribution_huge: round(sqrt(lambda) * N + lambda).
+__device__ __forceinline__ uint32_t poisson_huge(uint32_t r, double sqrt_lambda, double lambda)
+{
+    const double nd = normal_from_u32_f64(r);
+    return (uint32_t)(long long)round(__dadd_rn(__dmul_rn(sqrt_lambda, nd), lambda));
+}
+
+// ---- functors: iw inputs (32-bit engine words) -> ow outputs of T ----
+// Naming follows the reference entry point they serve.
+
+struct FnUint // uniform_distribution<uint> (uniform.hpp:42-53)
+{
+    using T                      = uint32_t;
+    static constexpr unsigned iw = 1, ow = 1;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const { out[0] = in[0]; }
+};
+
+struct FnUchar // uniform_distribution<uchar> (uniform.hpp:55-66): the word's 4 bytes
+{
+    using T                      = uint8_t;
+    static constexpr unsigned iw = 1, ow = 4;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = (uint8_t)in[0];
+        out[1] = (uint8_t)(in[0] >> 8);
+        out[2] = (uint8_t)(in[0] >> 16);
+        out[3] = (uint8_t)(in[0] >> 24);
+    }
+};
+
+struct FnUshort // uniform_distribution<ushort> (uniform.hpp:68-79): the word's 2 halves
+{
+    using T                      = uint16_t;
+    static constexpr unsigned iw = 1, ow = 2;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = (uint16_t)in[0];
+        out[1] = (uint16_t)(in[0] >> 16);
+    }
+};
+
+struct FnFloat // uniform_distribution<float> (uniform.hpp:81-91)
+{
+    using T                      = float;
+    static constexpr unsigned iw = 1, ow = 1;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = u32_to_f32(in[0]);
+    }
+};
+
+struct FnDouble // uniform_distribution<double> (uniform.hpp:93-103)
+{
+    using T                      = double;
+    static constexpr unsigned iw = 2, ow = 1;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = u32x2_to_f64(in[0], in[1]);
+    }
+};
+
+struct FnHalf // uniform_distribution<half> (uniform.hpp:105-117)
+{
+    using T                      = __half;
+    static constexpr unsigned iw = 1, ow = 2;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = u16_to_f16(in[0] & 0xffffu);
+        out[1] = u16_to_f16(in[0] >> 16);
+    }
+};
+
+struct FnNormalF // normal_distribution<float, uint, 4> (normal.hpp:49-69)
+{
+    using T                      = float;
+    static constexpr unsigned iw = 2, ow = 2;
+    float                     mean, stddev;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const float2 v = box_muller_f32(in[0], in[1]);
+        out[0]         = __fadd_rn(mean, __fmul_rn(v.x, stddev));
+        out[1]         = __fadd_rn(mean, __fmul_rn(v.y, stddev));
+    }
+};
+
+struct FnLogNormalF // log_normal_distribution<float, uint, 4> (log_normal.hpp:51-71)
+{
+    using T                      = float;
+    static constexpr unsigned iw = 2, ow = 2;
+    float                     mean, stddev;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const float2 v = box_muller_f32(in[0], in[1]);
+        out[0]         = expf(__fadd_rn(mean, __fmul_rn(v.x, stddev)));
+        out[1]         = expf(__fadd_rn(mean, __fmul_rn(v.y, stddev)));
+    }
+};
+
+struct FnNormalD // normal_distribution<double, uint, 4> (normal.hpp:90-111)
+{
+    using T                      = double;
+    static constexpr unsigned iw = 4, ow = 2;
+    double                    mean, stddev;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const double2 v = box_muller_f64(in[0], in[1], in[2], in[3]);
+        out[0]          = __dadd_rn(mean, __dmul_rn(v.x, stddev));
+        out[1]          = __dadd_rn(mean, __dmul_rn(v.y, stddev));
+    }
+};
+
+struct FnLogNormalD // log_normal_distribution<double, uint, 4> (log_normal.hpp:92-113)
+{
+    using T                      = double;
+    static constexpr unsigned iw = 4, ow = 2;
+    double                    mean, stddev;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const double2 v = box_muller_f64(in[0], in[1], in[2], in[3]);
+        out[0]          = exp(__dadd_rn(mean, __dmul_rn(v.x, stddev)));
+        out[1]          = exp(__dadd_rn(mean, __dmul_rn(v.y, stddev)));
+    }
+};
+
+struct FnNormalH // normal_distribution<half, uint, 4> (normal.hpp:113-136), float branch
+{
+    using T                      = __half;
+    static constexpr unsigned iw = 1, ow = 2;
+    float                     mean, stddev; // the half parameters widened to float
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        __half r[2];
+        box_muller_f16(in[0], r);
+        out[0] = __float2half_rn(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[0]))));
+        out[1] = __float2half_rn(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[1]))));
+    }
+};
+
+struct FnLogNormalH // log_normal_distribution<half, uint, 4> (log_normal.hpp:115-139)
+{
+    using T                      = __half;
+    static constexpr unsigned iw = 1, ow = 2;
+    float                     mean, stddev;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        __half r[2];
+        box_muller_f16(in[0], r);
+        out[0] = __float2half_rn(expf(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[0])))));
+        out[1] = __float2half_rn(expf(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[1])))));
+    }
+};
+
+// poisson_distribution<ALIAS> (poisson.hpp:49-76).  The table is staged in shared memory
+// by the kernel; prob/alias then point there.
+struct FnPoisson
+{
+    using T                      = uint32_t;
+    static constexpr unsigned iw = 1, ow = 1;
+    static constexpr bool     kTable = true;
+    const double*             prob;
+    const uint32_t*           alias;
+    uint32_t                  size, offset;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = alias_lookup(in[0], size, offset, prob, alias);
+    }
+};
+
+// poisson_distribution_huge (poisson.hpp:80-108), lambda > 4000.
+struct FnPoissonHuge
+{
+    using T                      = uint32_t;
+    static constexpr unsigned iw = 1, ow = 1;
+    double                    sqrt_lambda, lambda;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = poisson_huge(in[0], sqrt_lambda, lambda);
+    }
+};
+
+template<class F>
+struct has_table
+{
+    static constexpr bool value = false;
+};
+template<>
+struct has_table<FnPoisson>
+{
+    static constexpr bool value = true;
+};
+
+// Stages a Poisson alias table into shared memory (all threads of the block take part)
+// and returns a functor reading it there.  smem holds size doubles then size uints.
+template<class F>
+__device__ __forceinline__ F stage_table(const F& f, unsigned char* smem)
+{
+    if constexpr(has_table<F>::value)
+    {
+        double*   p = reinterpret_cast<double*>(smem);
+        uint32_t* a = reinterpret_cast<uint32_t*>(smem + sizeof(double) * f.size);
+        for(uint32_t i = threadIdx.x; i < f.size; i += blockDim.x)
+        {
+            p[i] = f.prob[i];
+            a[i] = f.alias[i];
+        }
+        __syncthreads();
+        F g     = f;
+        g.prob  = p;
+        g.alias = a;
+        return g;
+    }
+    else
+    {
+        return f;
+    }
+}
+
+template<class F>
+inline size_t table_smem_bytes(const F& f)
+{
+    if constexpr(has_table<F>::value)
+        return (size_t)f.size * (sizeof(double) + sizeof(uint32_t));
+    else
+        return 0;
+}
+
+// Calls `body(functor)` with the functor that serves distribution d.  Used by every
+// generator family to instantiate its kernel once per distribution.
+template<class Body>
+inline rocrand_status with_functor(Dist d, const DistParams& p, Body&& body)
+{
+    switch(d)
+    {
+        case Dist::U32: return body(FnUint{});
+        case Dist::U8: return body(FnUchar{});
+        case Dist::U16: return body(FnUshort{});
+        case Dist::F32: return body(FnFloat{});
+        case Dist::F64: return body(FnDouble{});
+        case Dist::F16: return body(FnHalf{});
+        case Dist::NORMAL_F32: return body(FnNormalF{p.mean_f, p.std_f});
+        case Dist::LOGNORMAL_F32: return body(FnLogNormalF{p.mean_f, p.std_f});
+        case Dist::NORMAL_F64: return body(FnNormalD{p.mean_d, p.std_d});
+        case Dist::LOGNORMAL_F64: return body(FnLogNormalD{p.mean_d, p.std_d});
+        case Dist::NORMAL_F16:
+            return body(FnNormalH{__half2float(__ushort_as_half(p.mean_h)),
+                                  __half2float(__ushort_as_half(p.std_h))});
+        case Dist::LOGNORMAL_F16:
+            return body(FnLogNormalH{__half2float(__ushort_as_half(p.mean_h)),
+                                     __half2float(__ushort_as_half(p.std_h))});
+        case Dist::POISSON:
+            if(p.huge)
+                return body(FnPoissonHuge{p.sqrt_lambda, p.lambda});
+            return body(FnPoisson{p.prob, p.alias, p.size, p.offset});
+        default: return ROCRAND_STATUS_TYPE_ERROR;
+    }
+}
+
+} // namespace rb200

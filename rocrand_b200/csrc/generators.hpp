@@ -1,0 +1,52 @@
+// generators.hpp -- generator objects behind the C ABI, one class per engine family.
+#pragma once
+
+#include "common.hpp"
+#include "counter_engines.cuh"
+#include "poisson.hpp"
+
+namespace rb200
+{
+
+// Common state of pseudo-random generators: seed, offset and ordering, with the
+// reference's lazy re-initialisation on any change (generator_type.hpp:235-291).
+class PseudoGeneratorBase : public rocrand_generator_base_type
+{
+public:
+    rocrand_status set_seed(unsigned long long seed) override
+    {
+        m_seed        = seed;
+        m_initialized = false;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+    rocrand_status set_offset(unsigned long long offset) override
+    {
+        m_offset      = offset;
+        m_initialized = false;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+protected:
+    unsigned long long m_seed        = 0;
+    unsigned long long m_offset      = 0;
+    rocrand_ordering   m_order       = ROCRAND_ORDERING_PSEUDO_DEFAULT;
+    bool               m_initialized = false;
+    PoissonCache       m_poisson;
+};
+
+class PhiloxGenerator final : public PseudoGeneratorBase
+{
+public:
+    PhiloxGenerator();
+    ~PhiloxGenerator() override;
+    rocrand_rng_type type() const override { return ROCRAND_RNG_PSEUDO_PHILOX4_32_10; }
+    rocrand_status   init() override;
+    rocrand_status   set_order(rocrand_ordering order) override;
+    rocrand_status   generate(void* data, size_t n, Dist d, const DistParams& p) override;
+    rocrand_status   generate_poisson(unsigned int* data, size_t n, double lambda) override;
+
+private:
+    CounterPos m_pos;
+};
+
+} // namespace rb200

@@ -1,0 +1,233 @@
+// philox.cu -- Philox4x32-10 generator: host object and fused sm_100a kernels.
+//
+// Output contract (what the reference's generate_philox, library/src/rng/philox4x32_10.hpp
+// :107-214, produces on its default 1024x256 grid), restated position by position so any
+// grid gives identical bytes:
+//   * the output is split into a head of `head` elements (up to the first 16-byte
+//     boundary), vec_n 16-byte vectors and a tail;
+//   * vector j holds the distribution applied to the 4 stream values starting at
+//     p(j) = 4*j + (j % 262144 == 0 ? start0 : head), where start0 = ceil(head/ow)*iw is
+//     how far the head moved thread 0 of the reference grid;
+//   * the head is produced sequentially from stream position 0, the tail sequentially
+//     from p(vec_n);
+//   * positions are relative to the generator's engine position, which advances by
+//     ceil(n/ow)*iw per call (philox4x32_10.hpp:349-354).
+// The common case (start0 == head and a block-aligned start) needs one Philox block per
+// vector; otherwise a vector straddles two blocks.
+#include "common.hpp"
+#include "counter_engines.cuh"
+#include "dist.cuh"
+#include "generators.hpp"
+#include "launch.cuh"
+#include "poisson.hpp"
+
+namespace rb200
+{
+
+struct PhiloxCall
+{
+    PhiloxKeys         keys;
+    uint4              c0;     // engine counter at the call's first value
+    uint32_t           s0;     // engine sub-position (0..3)
+    uint32_t           head;   // elements before the first 16-byte boundary
+    uint32_t           start0; // stream offset of vector 0 (thread 0 after the head)
+    uint32_t           tail;   // elements after the last full vector
+    unsigned char*     data;   // output base
+    unsigned char*     vec;    // first 16-byte aligned output byte
+    unsigned long long n;
+    unsigned long long vec_n;
+};
+
+// Value at relative stream position p (sequential head/tail path only).
+__device__ __forceinline__ uint32_t philox_value(const PhiloxCall& a, unsigned long long p)
+{
+    const unsigned long long q = a.s0 + p;
+    const uint4              b = philox_block(ctr_add(a.c0, q >> 2), a.keys);
+    return word_of(b, static_cast<uint32_t>(q & 3));
+}
+
+// Applies F sequentially from stream position `pos` and writes `count` elements at `out`
+// (the reference's scalar head/tail loops, one engine() per input).
+template<class F>
+__device__ void philox_scalar_run(const PhiloxCall& a, const F& f, unsigned long long pos,
+                                  typename F::T* out, uint32_t count)
+{
+    typename F::T v[F::ow];
+    uint32_t      in[F::iw];
+    for(uint32_t done = 0; done < count; done += F::ow)
+    {
+        for(unsigned i = 0; i < F::iw; i++)
+            in[i] = philox_value(a, pos++);
+        f(in, v);
+        for(unsigned o = 0; o < F::ow && done + o < count; o++)
+            out[done + o] = v[o];
+    }
+}
+
+template<class F>
+__device__ __forceinline__ uint4 philox_vec(const F& f, uint4 w)
+{
+    constexpr unsigned opt = 4 / F::iw;
+    typename F::T      out[opt * F::ow];
+    const uint32_t     in[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for(unsigned s = 0; s < opt; s++)
+        f(in + s * F::iw, out + s * F::ow);
+    return pack16(out);
+}
+
+// kAligned: start0 == head and (s0 + head) % 4 == 0, so vector j is exactly block
+// c0 + (s0 + head)/4 + j.
+template<class F, bool kAligned>
+__global__ void __launch_bounds__(kBlock) philox_fill(PhiloxCall a, F f)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const F g = stage_table(f, smem);
+
+    const unsigned long long tid    = static_cast<unsigned long long>(blockIdx.x) * kBlock + threadIdx.x;
+    const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * kBlock;
+
+    if(kAligned)
+    {
+        const uint4 cbase = ctr_add(a.c0, (a.s0 + a.head) >> 2);
+        for(unsigned long long j = tid; j < a.vec_n; j += stride)
+        {
+            const uint4 b = philox_block(ctr_add(cbase, j), a.keys);
+            store16_cs(a.vec + j * 16, philox_vec(g, b));
+        }
+    }
+    else
+    {
+        for(unsigned long long j = tid; j < a.vec_n; j += stride)
+        {
+            const uint32_t adj = (j & (kPhiloxRefStride - 1)) == 0 ? a.start0 : a.head;
+            const unsigned long long q = a.s0 + adj + 4 * j;
+            const uint4 c  = ctr_add(a.c0, q >> 2);
+            const uint32_t s = static_cast<uint32_t>(q & 3);
+            uint4 b = philox_block(c, a.keys);
+            if(s != 0)
+                b = interleave4(b, philox_block(ctr_add(c, 1), a.keys), s);
+            store16_cs(a.vec + j * 16, philox_vec(g, b));
+        }
+    }
+
+    if(tid == 0)
+    {
+        using T = typename F::T;
+        if(a.head > 0)
+            philox_scalar_run(a, g, 0, reinterpret_cast<T*>(a.data), a.head);
+        if(a.tail > 0)
+        {
+            const unsigned long long pos
+                = 4 * a.vec_n + ((a.vec_n % kPhiloxRefStride) == 0 ? a.start0 : a.head);
+            philox_scalar_run(a, g, pos, reinterpret_cast<T*>(a.data) + (a.n - a.tail), a.tail);
+        }
+    }
+}
+
+template<class F>
+static rocrand_status launch_philox(PhiloxCall a, const F& f, cudaStream_t stream)
+{
+    const size_t smem    = table_smem_bytes(f);
+    const bool   aligned = a.start0 == a.head && ((a.s0 + a.head) & 3u) == 0;
+    const unsigned long long work = a.vec_n > 0 ? a.vec_n : 1;
+    if(aligned)
+    {
+        auto k = philox_fill<F, true>;
+        k<<<grid_for(k, work, smem), kBlock, smem, stream>>>(a, f);
+    }
+    else
+    {
+        auto k = philox_fill<F, false>;
+        k<<<grid_for(k, work, smem), kBlock, smem, stream>>>(a, f);
+    }
+    return launch_status();
+}
+
+// ---------------------------------------------------------------------------------------
+
+PhiloxGenerator::PhiloxGenerator() = default;
+PhiloxGenerator::~PhiloxGenerator() = default;
+
+rocrand_status PhiloxGenerator::init()
+{
+    if(m_initialized)
+        return ROCRAND_STATUS_SUCCESS;
+    // seed(seed, subsequence 0, offset) (philox4x32_10.hpp:291-306, engine seed :134-141)
+    m_pos = CounterPos{};
+    m_pos.advance(m_offset);
+    m_initialized = true;
+    return ROCRAND_STATUS_SUCCESS;
+}
+
+rocrand_status PhiloxGenerator::set_order(rocrand_ordering order)
+{
+    // philox4x32_10.hpp:258-278: DEFAULT, DYNAMIC, BEST, LEGACY.  All give the same
+    // output on this build.
+    switch(order)
+    {
+        case ROCRAND_ORDERING_PSEUDO_DEFAULT:
+        case ROCRAND_ORDERING_PSEUDO_DYNAMIC:
+        case ROCRAND_ORDERING_PSEUDO_BEST:
+        case ROCRAND_ORDERING_PSEUDO_LEGACY:
+            m_order       = order;
+            m_initialized = false;
+            return ROCRAND_STATUS_SUCCESS;
+        default: return ROCRAND_STATUS_OUT_OF_RANGE;
+    }
+}
+
+rocrand_status PhiloxGenerator::generate(void* data, size_t n, Dist d, const DistParams& p)
+{
+    if(d == Dist::U64)
+        return ROCRAND_STATUS_TYPE_ERROR; // 32-bit engine (philox4x32_10.hpp:359-375)
+    rocrand_status st = init();
+    if(st != ROCRAND_STATUS_SUCCESS)
+        return st;
+    if(data == nullptr)
+        return ROCRAND_STATUS_SUCCESS;
+    const size_t tsize = dist_elem_size(d);
+    if(reinterpret_cast<uintptr_t>(data) % tsize != 0)
+        return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE; // not even element-aligned
+
+    st = with_functor(d, p, [&](auto f) -> rocrand_status {
+        using F                    = decltype(f);
+        constexpr unsigned iw      = F::iw;
+        constexpr unsigned ow      = F::ow;
+        constexpr unsigned fow     = (4 / iw) * ow; // elements per 16-byte vector
+        const uintptr_t    addr    = reinterpret_cast<uintptr_t>(data);
+        const size_t       mis     = (fow - addr / tsize % fow) % fow;
+        PhiloxCall         a;
+        a.keys   = philox_keys(m_seed);
+        a.c0     = m_pos.counter;
+        a.s0     = m_pos.sub;
+        a.head   = static_cast<uint32_t>(n < mis ? n : mis);
+        a.tail   = static_cast<uint32_t>((n - a.head) % fow);
+        a.vec_n  = (n - a.head) / fow;
+        a.start0 = a.head > 0 ? (a.head + ow - 1) / ow * iw : 0;
+        a.n      = n;
+        a.data   = static_cast<unsigned char*>(data);
+        a.vec    = a.data + mis * tsize;
+        if(n == 0)
+            return ROCRAND_STATUS_SUCCESS;
+        const rocrand_status s = launch_philox(a, f, m_stream);
+        if(s == ROCRAND_STATUS_SUCCESS)
+            m_pos.advance(static_cast<unsigned long long>((n + ow - 1) / ow) * iw);
+        return s;
+    });
+    return st;
+}
+
+rocrand_status PhiloxGenerator::generate_poisson(unsigned int* data, size_t n, double lambda)
+{
+    rocrand_status st = init();
+    if(st != ROCRAND_STATUS_SUCCESS)
+        return st;
+    DistParams p;
+    st = m_poisson.get(lambda, m_stream, false, p);
+    if(st != ROCRAND_STATUS_SUCCESS)
+        return st;
+    return generate(data, n, Dist::POISSON, p);
+}
+
+} // namespace rb200

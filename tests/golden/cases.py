@@ -1,0 +1,43 @@
+"""Call sequences recorded in the golden fixtures (see make_golden.py).
+
+A case is {"rng": type, "seed": s, "offset": o, "calls": [[dist, n, params, mis], ...]}.
+``mis`` places the output (mis * element size) mod 16 bytes past a 16-byte boundary, which
+selects the reference's head/tail split.  Sequences of several calls pin continuity.
+"""
+
+PSEUDO_DISTS = [
+    ("uint", []), ("char", []), ("short", []), ("uniform", []), ("uniform_double", []),
+    ("uniform_half", []), ("normal", [0.5, 2.0]), ("normal_double", [-1.0, 0.5]),
+    ("normal_half", [1.0, 2.0]), ("log_normal", [0.2, 0.7]), ("log_normal_double", [0.1, 0.4]),
+    ("log_normal_half", [0.0, 0.5]), ("poisson", [0.5]), ("poisson", [10.0]),
+    ("poisson", [1000.0]), ("poisson", [5000.5]),
+]
+
+
+def _seq(dist, params):
+    return [[dist, 1000, params, 0], [dist, 37, params, 1], [dist, 4099, params, 3],
+            [dist, 1, params, 2], [dist, 0, params, 0], [dist, 257, params, 5]]
+
+
+def pseudo_cases(rng, seeds_offsets, extra=()):
+    out = []
+    for seed, offset in seeds_offsets:
+        for dist, params in PSEUDO_DISTS:
+            out.append({"rng": rng, "seed": seed, "offset": offset, "calls": _seq(dist, params)})
+    out.extend(extra)
+    return out
+
+
+# Philox / ThreeFry: the vector at j % 262144 == 0 comes from thread 0 of the reference
+# grid, which the head moved by ceil(head/ow)*iw instead of head: pin that with a call
+# whose vector count is a multiple of 262144 (char: 16 per vector, 13 head elements).
+_STRIDE_CORNER = [
+    {"rng": 404, "seed": 77, "offset": 0,
+     "calls": [["char", 13 + 262144 * 16 + 5, [], 3], ["short", 7 + 262144 * 8 + 3, [], 1],
+               ["normal", 3 + 262144 * 4 + 1, [0.0, 1.0], 1]]},
+]
+
+CASES = {
+    "philox": pseudo_cases(404, [(1234, 0), (0xdeadbeef, 12345), (0xAAAAAAAAAAA, 2**40 + 3)],
+                           _STRIDE_CORNER),
+}

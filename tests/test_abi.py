@@ -1,0 +1,98 @@
+"""The drop-in boundary on CPU: librocrand.so loads, exports every entry point that
+include/rocrand/rocrand.h declares, and the host-side status logic matches the reference's
+library/src/rocrand.cpp (no kernel is launched here)."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+import rocrand_b200 as rb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in ("rocrand.h",):
+        with open(os.path.join(ROOT, "include", "rocrand", h)) as f:
+            text = f.read()
+        names |= set(re.findall(r"\b(rocrand_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(lib):
+    decl = declared_functions()
+    assert len(decl) >= 33
+    missing = [n for n in decl if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version(lib):
+    assert rb.get_version() == 300200
+
+
+def _create(lib, t):
+    g = ctypes.c_void_p()
+    st = lib.rocrand_create_generator(ctypes.byref(g), t)
+    return st, g
+
+
+def test_null_generator_is_not_created(lib):
+    null = ctypes.c_void_p(0)
+    assert lib.rocrand_generate(null, None, 0) == rb.ROCRAND_STATUS_NOT_CREATED
+    assert lib.rocrand_generate_uniform(null, None, 0) == rb.ROCRAND_STATUS_NOT_CREATED
+    assert lib.rocrand_set_seed(null, 1) == rb.ROCRAND_STATUS_NOT_CREATED
+    assert lib.rocrand_set_offset(null, 1) == rb.ROCRAND_STATUS_NOT_CREATED
+    assert lib.rocrand_set_ordering(null, 101) == rb.ROCRAND_STATUS_NOT_CREATED
+    assert lib.rocrand_generate_poisson(null, None, 0, 1.0) == rb.ROCRAND_STATUS_NOT_CREATED
+    assert lib.rocrand_initialize_generator(null) == rb.ROCRAND_STATUS_NOT_CREATED
+
+
+def test_unknown_type_is_type_error(lib):
+    st, _ = _create(lib, 12345)
+    assert st == rb.ROCRAND_STATUS_TYPE_ERROR
+
+
+def test_version_null_pointer(lib):
+    assert lib.rocrand_get_version(None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+
+
+@pytest.mark.parametrize("rng", [rb.ROCRAND_RNG_PSEUDO_PHILOX4_32_10])
+def test_host_side_semantics(lib, rng):
+    st, g = _create(lib, rng)
+    assert st == 0
+    try:
+        # lambda <= 0 is rejected before any work (rocrand.cpp:371-374)
+        assert lib.rocrand_generate_poisson(g, None, 10, 0.0) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+        assert lib.rocrand_generate_poisson(g, None, 10, -1.0) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+        # 64-bit output from a 32-bit engine (philox4x32_10.hpp:359-375)
+        assert lib.rocrand_generate_long_long(g, None, 10) == rb.ROCRAND_STATUS_TYPE_ERROR
+        # orderings: quasi ordering and SEEDED are refused by Philox
+        assert lib.rocrand_set_ordering(g, rb.ROCRAND_ORDERING_QUASI_DEFAULT) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+        assert lib.rocrand_set_ordering(g, rb.ROCRAND_ORDERING_PSEUDO_SEEDED) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+        for o in (100, 101, 103, 104):
+            assert lib.rocrand_set_ordering(g, o) == 0
+        # pseudo generators have no dimensions and no uint4 seed
+        assert lib.rocrand_set_quasi_random_generator_dimensions(g, 4) == rb.ROCRAND_STATUS_TYPE_ERROR
+        assert lib.rocrand_set_seed_uint4(g, rb._Uint4(1, 2, 3, 4)) == rb.ROCRAND_STATUS_TYPE_ERROR
+        # a NULL output pointer initialises and returns SUCCESS (philox4x32_10.hpp:323-326)
+        assert lib.rocrand_set_seed(g, 5) == 0
+        assert lib.rocrand_set_offset(g, 17) == 0
+        assert lib.rocrand_generate_uniform(g, None, 100) == 0
+        assert lib.rocrand_initialize_generator(g) == 0
+    finally:
+        assert lib.rocrand_destroy_generator(g) == 0
+
+
+def test_discrete_null_arguments(lib):
+    lib.rocrand_create_poisson_distribution.argtypes = [ctypes.c_double, ctypes.c_void_p]
+    lib.rocrand_create_discrete_distribution.argtypes = [ctypes.c_void_p, ctypes.c_uint,
+                                                        ctypes.c_uint, ctypes.c_void_p]
+    lib.rocrand_destroy_discrete_distribution.argtypes = [ctypes.c_void_p]
+    out = ctypes.c_void_p()
+    assert lib.rocrand_create_poisson_distribution(1.0, None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+    assert lib.rocrand_create_poisson_distribution(0.0, ctypes.byref(out)) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+    assert lib.rocrand_create_discrete_distribution(None, 0, 0, ctypes.byref(out)) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+    assert lib.rocrand_destroy_discrete_distribution(None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
