@@ -12,7 +12,11 @@ static int is_supported(int t)
 {
     switch(t)
     {
-        case ORC_RNG_PHILOX: return 1;
+        case ORC_RNG_PHILOX:
+        case ORC_RNG_THREEFRY2_32:
+        case ORC_RNG_THREEFRY2_64:
+        case ORC_RNG_THREEFRY4_32:
+        case ORC_RNG_THREEFRY4_64: return 1;
         default: return 0;
     }
 }
@@ -63,6 +67,10 @@ int orc_initialize(orc_gen* g)
     switch(g->rng_type)
     {
         case ORC_RNG_PHILOX: orc_philox_seed(&g->st.philox, g->seed, 0, g->offset); break;
+        case ORC_RNG_THREEFRY2_32: orc_threefry_seed(&g->st.threefry, 2, 32, g->seed, g->offset); break;
+        case ORC_RNG_THREEFRY2_64: orc_threefry_seed(&g->st.threefry, 2, 64, g->seed, g->offset); break;
+        case ORC_RNG_THREEFRY4_32: orc_threefry_seed(&g->st.threefry, 4, 32, g->seed, g->offset); break;
+        case ORC_RNG_THREEFRY4_64: orc_threefry_seed(&g->st.threefry, 4, 64, g->seed, g->offset); break;
         default: return ORC_TYPE_ERROR;
     }
     g->initialized = 1;
@@ -135,18 +143,38 @@ int orc_set_dimensions(orc_gen* g, unsigned int dims)
 
 /* ---- generate dispatch ---- */
 
-static int run(orc_gen* g, void* data, size_t n, const orc_dist* d)
+static int is_threefry64(int t) { return t == ORC_RNG_THREEFRY2_64 || t == ORC_RNG_THREEFRY4_64; }
+static int is_threefry(int t)
 {
+    return t == ORC_RNG_THREEFRY2_32 || t == ORC_RNG_THREEFRY4_32 || is_threefry64(t);
+}
+
+static int run(orc_gen* g, void* data, size_t n, const orc_dist* din)
+{
+    orc_dist d = *din;
+    /* 64-bit output only from 64-bit engines (philox4x32_10.hpp:359-375, threefry.hpp:316-321) */
+    if(d.kind == D_ULL && !is_threefry64(g->rng_type))
+        return ORC_TYPE_ERROR;
+    if(is_threefry64(g->rng_type))
+        orc_dist_to64(&d);
+    /* ThreeFry2x32 serves double normals with the one-word functor (threefry.hpp:441-449) */
+    if(g->rng_type == ORC_RNG_THREEFRY2_32 && (d.kind == D_NORMAL_D || d.kind == D_LOGNORMAL_D))
+    {
+        const double m = d.mean_d, s = d.std_d;
+        orc_dist_init(&d, d.kind == D_NORMAL_D ? D_NORMAL_D1 : D_LOGNORMAL_D1);
+        d.mean_d = m;
+        d.std_d  = s;
+    }
     int st = orc_initialize(g);
     if(st != ORC_SUCCESS)
         return st;
     if(data == NULL)
         return ORC_SUCCESS;
-    switch(g->rng_type)
-    {
-        case ORC_RNG_PHILOX: return orc_philox_generate(g, data, n, d);
-        default: return ORC_TYPE_ERROR;
-    }
+    if(g->rng_type == ORC_RNG_PHILOX)
+        return orc_philox_generate(g, data, n, &d);
+    if(is_threefry(g->rng_type))
+        return orc_threefry_generate(g, data, n, &d);
+    return ORC_TYPE_ERROR;
 }
 
 static int run_kind(orc_gen* g, void* data, size_t n, orc_dist_kind k)
@@ -162,10 +190,7 @@ int orc_generate(orc_gen* g, uint32_t* out, size_t n) { return run_kind(g, out, 
 
 int orc_generate_long_long(orc_gen* g, uint64_t* out, size_t n)
 {
-    (void)out, (void)n;
-    if(!g)
-        return ORC_NOT_CREATED;
-    return ORC_TYPE_ERROR;
+    return run_kind(g, out, n, D_ULL);
 }
 
 int orc_generate_char(orc_gen* g, uint8_t* out, size_t n) { return run_kind(g, out, n, D_UCHAR); }

@@ -186,6 +186,7 @@ void orc_dist_init(orc_dist* d, orc_dist_kind kind)
         case D_POISSON_HUGE: d->iw = 1; d->ow = 1; d->tsize = 4; break;
         case D_NORMAL_D1:
         case D_LOGNORMAL_D1: d->iw = 1; d->ow = 1; d->tsize = 8; break;
+        case D_ULL: d->iw = 1; d->ow = 1; d->tsize = 8; break;
     }
 }
 
@@ -296,6 +297,7 @@ void orc_dist_apply(const orc_dist* d, const uint32_t* in, void* outv)
             o[0]      = exp(d->mean_d + normal_d1(in[0]) * d->std_d);
             break;
         }
+        case D_ULL: break;
     }
 }
 
@@ -442,4 +444,130 @@ void orc_poisson_free(orc_poisson* pm)
     free(pm->prob);
     free(pm->alias);
     memset(pm, 0, sizeof(*pm));
+}
+
+/* ---- 64-bit engine words (uniform.hpp:119-200, normal.hpp:138-200, log_normal.hpp:138-200,
+ *      rocrand_uniform.h:66-69,109-116, rocrand_normal.h:53-58,81-89,124-129,
+ *      rocrand_discrete.h:75-81) ---- */
+
+void orc_dist_to64(orc_dist* d)
+{
+    switch(d->kind)
+    {
+        case D_ULL: d->iw = 1; d->ow = 1; d->tsize = 8; break;
+        case D_UINT: d->iw = 1; d->ow = 2; break;
+        case D_UCHAR: d->iw = 1; d->ow = 8; break;
+        case D_USHORT: d->iw = 1; d->ow = 4; break;
+        case D_FLOAT: d->iw = 1; d->ow = 1; break;
+        case D_DOUBLE: d->iw = 1; d->ow = 1; break;
+        case D_HALF: d->iw = 1; d->ow = 4; break;
+        case D_NORMAL_F:
+        case D_LOGNORMAL_F: d->iw = 1; d->ow = 2; break;
+        case D_NORMAL_D:
+        case D_LOGNORMAL_D: d->iw = 2; d->ow = 2; break;
+        case D_NORMAL_H:
+        case D_LOGNORMAL_H: d->iw = 1; d->ow = 2; break;
+        default: break; /* Poisson: iw1 ow1 */
+    }
+}
+
+static double uniform_d64(uint64_t v)
+{
+    return ORC_2POW53_INV_DOUBLE + ((v >> 11) * ORC_2POW53_INV_DOUBLE);
+}
+
+void orc_dist_apply64(const orc_dist* d, const uint64_t* in, void* outv)
+{
+    switch(d->kind)
+    {
+        case D_ULL:
+        case D_UINT:
+        case D_UCHAR:
+        case D_USHORT: memcpy(outv, &in[0], 8); break;
+        case D_FLOAT:
+        {
+            float* o = (float*)outv;
+            o[0]     = ORC_2POW32_INV + ((in[0] >> 32) * ORC_2POW32_INV);
+            break;
+        }
+        case D_DOUBLE:
+        {
+            double* o = (double*)outv;
+            o[0]      = uniform_d64(in[0]);
+            break;
+        }
+        case D_HALF:
+        {
+            uint16_t* o = (uint16_t*)outv;
+            for(int k = 0; k < 4; k++)
+                o[k] = uniform_h((uint16_t)(in[0] >> (16 * k)));
+            break;
+        }
+        case D_NORMAL_F:
+        case D_LOGNORMAL_F:
+        {
+            float  r[2];
+            float* o = (float*)outv;
+            box_muller_f((uint32_t)in[0], (uint32_t)(in[0] >> 32), r);
+            for(int k = 0; k < 2; k++)
+            {
+                const float z = d->mean_f + r[k] * d->std_f;
+                o[k]          = d->kind == D_NORMAL_F ? z : expf(z);
+            }
+            break;
+        }
+        case D_NORMAL_D:
+        case D_LOGNORMAL_D:
+        {
+            double  r[2];
+            double* o = (double*)outv;
+            box_muller_d((uint32_t)in[0], (uint32_t)(in[0] >> 32), (uint32_t)in[1],
+                         (uint32_t)(in[1] >> 32), r);
+            for(int k = 0; k < 2; k++)
+            {
+                const double z = d->mean_d + r[k] * d->std_d;
+                o[k]           = d->kind == D_NORMAL_D ? z : exp(z);
+            }
+            break;
+        }
+        case D_NORMAL_H:
+        case D_LOGNORMAL_H:
+        {
+            uint16_t  r[2];
+            uint16_t* o = (uint16_t*)outv;
+            box_muller_h((uint16_t)in[0], (uint16_t)(in[0] >> 32), r);
+            const float m = orc_half_to_float(d->mean_h);
+            const float s = orc_half_to_float(d->std_h);
+            for(int k = 0; k < 2; k++)
+            {
+                const float z = m + (s * orc_half_to_float(r[k]));
+                o[k]          = orc_float_to_half(d->kind == D_NORMAL_H ? z : expf(z));
+            }
+            break;
+        }
+        case D_POISSON:
+        {
+            /* x = r * 2^-64; r rounds to double first.  When it rounds up to 2^64 the
+             * reference indexes one past the table; the index is clamped here. */
+            uint32_t*      o   = (uint32_t*)outv;
+            const double   x   = in[0] * ORC_2POW64_INV_DOUBLE;
+            const double   nx  = d->size * x;
+            const double   fnx = floor(nx);
+            const double   y   = nx - fnx;
+            uint32_t       i   = (uint32_t)fnx;
+            if(i >= d->size)
+                i = d->size - 1;
+            o[0] = d->offset + (y < d->prob[i] ? i : d->alias[i]);
+            break;
+        }
+        case D_POISSON_HUGE:
+        {
+            uint32_t*    o  = (uint32_t*)outv;
+            const double p  = uniform_d64(in[0]);
+            const double nd = (double)ORC_SQRT2 * erfinv_d(2.0 * p - 1.0);
+            o[0]            = (uint32_t)round(d->sqrt_lambda * nd + d->lambda);
+            break;
+        }
+        default: break;
+    }
 }

@@ -87,7 +87,8 @@ typedef enum {
     D_POISSON,      /* poisson_distribution<ALIAS>       iw1 ow1 (poisson.hpp:49-76)  */
     D_POISSON_HUGE, /* poisson_distribution_huge         iw1 ow1 (poisson.hpp:80-108) */
     D_NORMAL_D1,    /* normal_distribution<double,u32,2> iw1 ow1 (normal.hpp:71-88)   */
-    D_LOGNORMAL_D1  /* log_normal_distribution<double,u32,2> iw1 ow1                  */
+    D_LOGNORMAL_D1, /* log_normal_distribution<double,u32,2> iw1 ow1                  */
+    D_ULL           /* uniform_distribution<ull,ull>     iw1 ow1 (uniform.hpp:119-130)*/
 } orc_dist_kind;
 
 typedef struct orc_dist {
@@ -108,6 +109,10 @@ typedef struct orc_dist {
 /* Applies a distribution to iw 32-bit engine outputs, writing ow values of tsize bytes. */
 void orc_dist_apply(const orc_dist* d, const uint32_t* in, void* out);
 void orc_dist_init(orc_dist* d, orc_dist_kind kind);
+/* The same distributions over 64-bit engine words (ThreeFry 2x64/4x64): uniform.hpp:119-200,
+ * normal.hpp:138-200, log_normal.hpp:138-200; iw/ow are re-set for 64-bit inputs. */
+void orc_dist_to64(orc_dist* d);
+void orc_dist_apply64(const orc_dist* d, const uint64_t* in, void* out);
 void orc_store(const orc_dist* d, void* data, size_t idx, const void* vals, unsigned k);
 
 /* Poisson cache per generator (poisson.hpp:171-412). */
@@ -138,6 +143,20 @@ void orc_philox_seed(orc_philox* e, unsigned long long seed, unsigned long long 
 void orc_philox_discard(orc_philox* e, unsigned long long offset);
 int  orc_philox_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
 
+/* ThreeFry engines (rocrand_threefry{2,4}_impl.h), words kept in 64-bit storage. */
+typedef struct {
+    int      dim;  /* 2 or 4 words per block */
+    int      bits; /* 32 or 64 */
+    uint64_t counter[4];
+    uint64_t key[4];
+    uint64_t result[4];
+    uint32_t substate;
+} orc_threefry;
+
+void orc_threefry_seed(orc_threefry* e, int dim, int bits, unsigned long long seed,
+                       unsigned long long offset);
+int  orc_threefry_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
+
 struct orc_gen {
     int                rng_type;
     int                order;
@@ -147,7 +166,8 @@ struct orc_gen {
     unsigned           dims;
     orc_poisson        poisson;
     union {
-        orc_philox philox;
+        orc_philox   philox;
+        orc_threefry threefry;
     } st;
 };
 

@@ -9,8 +9,8 @@ Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline / reference
 import this module, and only as the checker or the timed CPU baseline.
 
 Alignment matters for parity: the reference derives its head/tail split from the output
-address, so every generate call here takes ``mis`` = (address mod 16) / element size and
-places the host output at exactly that alignment.
+address (vectors of 8 to 32 bytes), so every generate call here takes ``mis`` and places
+the host output (mis * element size) mod 64 bytes past a 64-byte boundary.
 """
 
 import ctypes
@@ -110,14 +110,14 @@ class CLib:
 
     def generate(self, g, dist, n, params=(), mis=0):
         """Returns (status, values) for one generate call with the output placed at
-        (mis * itemsize) mod 16 bytes past a 16-byte boundary."""
+        (mis * itemsize) mod 64 bytes past a 64-byte boundary."""
         suffix, dt, _ = DISTS[dist]
         isz = np.dtype(dt).itemsize
-        buf = np.zeros(n + 64 // isz + 16, dtype=dt)
+        buf = np.zeros(n + 128 // isz + 16, dtype=dt)
         base = buf.ctypes.data
-        want = (mis * isz) % 16
+        want = (mis * isz) % 64
         off = 0
-        while (base + off * isz) % 16 != want:
+        while (base + off * isz) % 64 != want:
             off += 1
         view = buf[off:off + n]
         st = self.fn(suffix)(g, c_void_p(view.ctypes.data), c_size_t(n), *dist_args(dist, params))

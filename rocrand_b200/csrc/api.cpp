@@ -41,6 +41,10 @@ static rocrand_generator_base_type* make_generator(rocrand_rng_type t)
     switch(t)
     {
         case ROCRAND_RNG_PSEUDO_PHILOX4_32_10: return new PhiloxGenerator();
+        case ROCRAND_RNG_PSEUDO_THREEFRY2_32_20:
+        case ROCRAND_RNG_PSEUDO_THREEFRY2_64_20:
+        case ROCRAND_RNG_PSEUDO_THREEFRY4_32_20:
+        case ROCRAND_RNG_PSEUDO_THREEFRY4_64_20: return make_threefry(t);
         default: return nullptr;
     }
 }

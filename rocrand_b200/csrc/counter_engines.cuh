@@ -57,6 +57,55 @@ __device__ __forceinline__ uint4 philox_block(uint4 c, const PhiloxKeys& pk)
     return c;
 }
 
+// Philox blocks of counters (x0 + i, y, z, w) with y, z, w fixed across a launch (no carry
+// out of the low word): the multiplies of rounds 1 and 2 whose operands are the fixed
+// words are evaluated once on the host, so a block costs 18 instead of 20 wide multiplies.
+struct PhiloxLane
+{
+    uint32_t a;    // round 1 word 0: hi(M1*z) ^ y ^ k0[0]
+    uint32_t b;    // round 1 word 1: lo(M1*z)
+    uint32_t wk;   // w ^ k0[1]
+    uint32_t hima; // hi(M0*a)
+    uint32_t loma; // lo(M0*a)
+};
+
+inline PhiloxLane philox_lane(uint4 c, const PhiloxKeys& pk)
+{
+    PhiloxLane     l;
+    const uint64_t p1 = static_cast<uint64_t>(kPhiloxM1) * c.z;
+    l.a               = static_cast<uint32_t>(p1 >> 32) ^ c.y ^ pk.k[0][0];
+    l.b               = static_cast<uint32_t>(p1);
+    l.wk              = c.w ^ pk.k[0][1];
+    const uint64_t pa = static_cast<uint64_t>(kPhiloxM0) * l.a;
+    l.hima            = static_cast<uint32_t>(pa >> 32);
+    l.loma            = static_cast<uint32_t>(pa);
+    return l;
+}
+
+__device__ __forceinline__ uint4 philox_block_lane(uint32_t x, const PhiloxLane& l,
+                                                   const PhiloxKeys& pk)
+{
+    // round 1: only M0 * x varies
+    const uint64_t p0 = static_cast<uint64_t>(kPhiloxM0) * x;
+    const uint32_t c2 = static_cast<uint32_t>(p0 >> 32) ^ l.wk;
+    const uint32_t d2 = static_cast<uint32_t>(p0);
+    // round 2: word 0 is the fixed `a`, so only M1 * c2 varies
+    const uint64_t p1 = static_cast<uint64_t>(kPhiloxM1) * c2;
+    uint4          c  = make_uint4(static_cast<uint32_t>(p1 >> 32) ^ l.b ^ pk.k[1][0],
+                                   static_cast<uint32_t>(p1), l.hima ^ d2 ^ pk.k[1][1], l.loma);
+#pragma unroll
+    for(int r = 2; r < 10; r++)
+    {
+        const uint64_t q0 = static_cast<uint64_t>(kPhiloxM0) * c.x;
+        const uint64_t q1 = static_cast<uint64_t>(kPhiloxM1) * c.z;
+        c = make_uint4(static_cast<uint32_t>(q1 >> 32) ^ c.y ^ pk.k[r][0],
+                       static_cast<uint32_t>(q1),
+                       static_cast<uint32_t>(q0 >> 32) ^ c.w ^ pk.k[r][1],
+                       static_cast<uint32_t>(q0));
+    }
+    return c;
+}
+
 // 128-bit counter + 64-bit addend, with carries (the engine's discard_state arithmetic).
 __host__ __device__ __forceinline__ uint4 ctr_add(uint4 c, uint64_t a)
 {

@@ -309,6 +309,169 @@ struct FnPoissonHuge
     }
 };
 
+// ---- functors over 64-bit engine words (ThreeFry 2x64/4x64) ----
+// uniform.hpp:119-200, normal.hpp:138-200, log_normal.hpp:138-200, and the 64-bit input
+// overloads of rocrand_uniform.h / rocrand_normal.h / rocrand_discrete.h.
+
+struct Fn64Ulonglong // uniform_distribution<ull, ull>
+{
+    using T                      = unsigned long long;
+    static constexpr unsigned iw = 1, ow = 1;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        out[0] = in[0];
+    }
+};
+
+template<class U, unsigned N>
+struct Fn64Split // uchar (ow 8), ushort (ow 4), uint (ow 2): the word's bytes in order
+{
+    using T                      = U;
+    static constexpr unsigned iw = 1, ow = N;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+#pragma unroll
+        for(unsigned k = 0; k < N; k++)
+            out[k] = static_cast<U>(in[0] >> (k * 8 * sizeof(U)));
+    }
+};
+
+struct Fn64Float // rocrand_uniform.h:66-69: 2^-32 + (v >> 32) * 2^-32
+{
+    using T                      = float;
+    static constexpr unsigned iw = 1, ow = 1;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        out[0] = u32_to_f32(static_cast<uint32_t>(in[0] >> 32));
+    }
+};
+
+struct Fn64Double // rocrand_uniform.h:109-116: 2^-53 + (v >> 11) * 2^-53
+{
+    using T                      = double;
+    static constexpr unsigned iw = 1, ow = 1;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        out[0] = __fma_rn(__ull2double_rn(in[0] >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+    }
+};
+
+struct Fn64Half // uniform_distribution<half, ull>: four 16-bit fields
+{
+    using T                      = __half;
+    static constexpr unsigned iw = 1, ow = 4;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+#pragma unroll
+        for(unsigned k = 0; k < 4; k++)
+            out[k] = u16_to_f16(static_cast<uint32_t>(in[0] >> (16 * k)) & 0xffffu);
+    }
+};
+
+struct Fn64NormalF // box_muller(unsigned long long): x = low word, y = high word
+{
+    using T                      = float;
+    static constexpr unsigned iw = 1, ow = 2;
+    float                     mean, stddev;
+    bool                      log_normal;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        const float2 v = box_muller_f32(static_cast<uint32_t>(in[0]), static_cast<uint32_t>(in[0] >> 32));
+        const float  a = __fadd_rn(mean, __fmul_rn(v.x, stddev));
+        const float  b = __fadd_rn(mean, __fmul_rn(v.y, stddev));
+        out[0]         = log_normal ? expf(a) : a;
+        out[1]         = log_normal ? expf(b) : b;
+    }
+};
+
+struct Fn64NormalD // box_muller_double(ulonglong2)
+{
+    using T                      = double;
+    static constexpr unsigned iw = 2, ow = 2;
+    double                    mean, stddev;
+    bool                      log_normal;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        const double2 v = box_muller_f64(static_cast<uint32_t>(in[0]), static_cast<uint32_t>(in[0] >> 32),
+                                         static_cast<uint32_t>(in[1]), static_cast<uint32_t>(in[1] >> 32));
+        const double  a = __dadd_rn(mean, __dmul_rn(v.x, stddev));
+        const double  b = __dadd_rn(mean, __dmul_rn(v.y, stddev));
+        out[0]          = log_normal ? exp(a) : a;
+        out[1]          = log_normal ? exp(b) : b;
+    }
+};
+
+struct Fn64NormalH // normal_distribution_half2(ull): (ushort)v and (ushort)(v >> 32)
+{
+    using T                      = __half;
+    static constexpr unsigned iw = 1, ow = 2;
+    float                     mean, stddev;
+    bool                      log_normal;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        __half         r[2];
+        const uint32_t v = (static_cast<uint32_t>(in[0]) & 0xffffu)
+                           | (static_cast<uint32_t>(in[0] >> 32) << 16);
+        box_muller_f16(v, r);
+#pragma unroll
+        for(int k = 0; k < 2; k++)
+        {
+            const float z = __fadd_rn(mean, __fmul_rn(stddev, __half2float(r[k])));
+            out[k]        = __float2half_rn(log_normal ? expf(z) : z);
+        }
+    }
+};
+
+// discrete_alias(unsigned long long) (rocrand_discrete.h:75-81): x = r * 2^-64 after the
+// round-to-nearest conversion of r to double.  When r rounds up to 2^64 the reference reads
+// one entry past the table; here the index is clamped to the last entry instead.
+struct Fn64Poisson
+{
+    using T                      = uint32_t;
+    static constexpr unsigned iw = 1, ow = 1;
+    const double*             prob;
+    const uint32_t*           alias;
+    uint32_t                  size, offset;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        const double x   = __dmul_rn(__ull2double_rn(in[0]), 5.4210108624275221700372640043497e-20);
+        const double nx  = __dmul_rn(__uint2double_rn(size), x);
+        const double fnx = floor(nx);
+        const double y   = __dsub_rn(nx, fnx);
+        uint32_t     i   = __double2uint_rz(fnx);
+        i                = i < size ? i : size - 1;
+        out[0]           = offset + (y < prob[i] ? i : alias[i]);
+    }
+};
+
+struct Fn64PoissonHuge // normal_distribution_double(ull) then round(sqrt(l) * N + l)
+{
+    using T                      = uint32_t;
+    static constexpr unsigned iw = 1, ow = 1;
+    double                    sqrt_lambda, lambda;
+    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    {
+        const double p  = __fma_rn(__ull2double_rn(in[0] >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+        const double nd = __dmul_rn((double)RB_SQRT2, erfinv_d(__dsub_rn(__dmul_rn(2.0, p), 1.0)));
+        out[0]          = (uint32_t)(long long)round(__dadd_rn(__dmul_rn(sqrt_lambda, nd), lambda));
+    }
+};
+
+// normal_distribution<double, uint, 2> / log_normal_distribution<double, uint, 2>
+// (normal.hpp:71-88): the inverse-erf normal, one word per value; used by ThreeFry2x32.
+struct FnNormalD1
+{
+    using T                      = double;
+    static constexpr unsigned iw = 1, ow = 1;
+    double                    mean, stddev;
+    bool                      log_normal;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const double z = __dadd_rn(mean, __dmul_rn(normal_from_u32_f64(in[0]), stddev));
+        out[0]         = log_normal ? exp(z) : z;
+    }
+};
+
 template<class F>
 struct has_table
 {
@@ -316,6 +479,11 @@ struct has_table
 };
 template<>
 struct has_table<FnPoisson>
+{
+    static constexpr bool value = true;
+};
+template<>
+struct has_table<Fn64Poisson>
 {
     static constexpr bool value = true;
 };
@@ -382,6 +550,35 @@ inline rocrand_status with_functor(Dist d, const DistParams& p, Body&& body)
             if(p.huge)
                 return body(FnPoissonHuge{p.sqrt_lambda, p.lambda});
             return body(FnPoisson{p.prob, p.alias, p.size, p.offset});
+        default: return ROCRAND_STATUS_TYPE_ERROR;
+    }
+}
+
+// Functor selection for engines producing 64-bit words.
+template<class Body>
+inline rocrand_status with_functor64(Dist d, const DistParams& p, Body&& body)
+{
+    const float mh = __half2float(__ushort_as_half(p.mean_h));
+    const float sh = __half2float(__ushort_as_half(p.std_h));
+    switch(d)
+    {
+        case Dist::U64: return body(Fn64Ulonglong{});
+        case Dist::U32: return body(Fn64Split<uint32_t, 2>{});
+        case Dist::U8: return body(Fn64Split<uint8_t, 8>{});
+        case Dist::U16: return body(Fn64Split<uint16_t, 4>{});
+        case Dist::F32: return body(Fn64Float{});
+        case Dist::F64: return body(Fn64Double{});
+        case Dist::F16: return body(Fn64Half{});
+        case Dist::NORMAL_F32: return body(Fn64NormalF{p.mean_f, p.std_f, false});
+        case Dist::LOGNORMAL_F32: return body(Fn64NormalF{p.mean_f, p.std_f, true});
+        case Dist::NORMAL_F64: return body(Fn64NormalD{p.mean_d, p.std_d, false});
+        case Dist::LOGNORMAL_F64: return body(Fn64NormalD{p.mean_d, p.std_d, true});
+        case Dist::NORMAL_F16: return body(Fn64NormalH{mh, sh, false});
+        case Dist::LOGNORMAL_F16: return body(Fn64NormalH{mh, sh, true});
+        case Dist::POISSON:
+            if(p.huge)
+                return body(Fn64PoissonHuge{p.sqrt_lambda, p.lambda});
+            return body(Fn64Poisson{p.prob, p.alias, p.size, p.offset});
         default: return ROCRAND_STATUS_TYPE_ERROR;
     }
 }

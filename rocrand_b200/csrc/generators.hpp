@@ -49,4 +49,7 @@ private:
     CounterPos m_pos;
 };
 
+// Factories of the other generator families (one translation unit each).
+rocrand_generator_base_type* make_threefry(rocrand_rng_type t);
+
 } // namespace rb200

@@ -125,6 +125,40 @@ __global__ void __launch_bounds__(kBlock) philox_fill(PhiloxCall a, F f)
     }
 }
 
+// Fast path: aligned vectors whose counters (x0 + j, y, z, w) share the upper words for the
+// whole launch (x0 + vec_n <= 2^32, checked by the host).  Each thread produces two
+// independent vectors per iteration so the two multiply chains interleave.
+template<class F>
+__global__ void __launch_bounds__(kBlock)
+    philox_fill_fast(PhiloxCall a, PhiloxLane lane, uint32_t x0, F f)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const F g = stage_table(f, smem);
+
+    const uint32_t vec_n  = static_cast<uint32_t>(a.vec_n);
+    const uint32_t stride = gridDim.x * kBlock;
+    uint32_t       j      = blockIdx.x * kBlock + threadIdx.x;
+    for(; j + stride < vec_n; j += 2 * stride)
+    {
+        const uint4 b0 = philox_block_lane(x0 + j, lane, a.keys);
+        const uint4 b1 = philox_block_lane(x0 + j + stride, lane, a.keys);
+        store16_cs(a.vec + static_cast<size_t>(j) * 16, philox_vec(g, b0));
+        store16_cs(a.vec + static_cast<size_t>(j + stride) * 16, philox_vec(g, b1));
+    }
+    if(j < vec_n)
+        store16_cs(a.vec + static_cast<size_t>(j) * 16, philox_vec(g, philox_block_lane(x0 + j, lane, a.keys)));
+
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        using T = typename F::T;
+        if(a.head > 0)
+            philox_scalar_run(a, g, 0, reinterpret_cast<T*>(a.data), a.head);
+        if(a.tail > 0)
+            philox_scalar_run(a, g, 4 * a.vec_n + a.head, reinterpret_cast<T*>(a.data) + (a.n - a.tail),
+                              a.tail);
+    }
+}
+
 template<class F>
 static rocrand_status launch_philox(PhiloxCall a, const F& f, cudaStream_t stream)
 {
@@ -133,6 +167,16 @@ static rocrand_status launch_philox(PhiloxCall a, const F& f, cudaStream_t strea
     const unsigned long long work = a.vec_n > 0 ? a.vec_n : 1;
     if(aligned)
     {
+        const uint4 cbase = ctr_add(a.c0, (a.s0 + a.head) >> 2);
+        // 32-bit indices in the fast kernel: keep j + 2*stride below 2^32 too.
+        if(static_cast<unsigned long long>(cbase.x) + a.vec_n <= (1ull << 32)
+           && a.vec_n < (1ull << 31))
+        {
+            const PhiloxLane lane = philox_lane(cbase, a.keys);
+            auto             k    = philox_fill_fast<F>;
+            k<<<grid_for(k, (work + 1) / 2, smem), kBlock, smem, stream>>>(a, lane, cbase.x, f);
+            return launch_status();
+        }
         auto k = philox_fill<F, true>;
         k<<<grid_for(k, work, smem), kBlock, smem, stream>>>(a, f);
     }

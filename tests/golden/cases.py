@@ -1,12 +1,12 @@
 """Call sequences recorded in the golden fixtures (see make_golden.py).
 
 A case is {"rng": type, "seed": s, "offset": o, "calls": [[dist, n, params, mis], ...]}.
-``mis`` places the output (mis * element size) mod 16 bytes past a 16-byte boundary, which
+``mis`` places the output (mis * element size) mod 64 bytes past a 64-byte boundary, which
 selects the reference's head/tail split.  Sequences of several calls pin continuity.
 """
 
 PSEUDO_DISTS = [
-    ("uint", []), ("char", []), ("short", []), ("uniform", []), ("uniform_double", []),
+    ("uint", []), ("ulonglong", []), ("char", []), ("short", []), ("uniform", []), ("uniform_double", []),
     ("uniform_half", []), ("normal", [0.5, 2.0]), ("normal_double", [-1.0, 0.5]),
     ("normal_half", [1.0, 2.0]), ("log_normal", [0.2, 0.7]), ("log_normal_double", [0.1, 0.4]),
     ("log_normal_half", [0.0, 0.5]), ("poisson", [0.5]), ("poisson", [10.0]),
@@ -37,7 +37,19 @@ _STRIDE_CORNER = [
                ["normal", 3 + 262144 * 4 + 1, [0.0, 1.0], 1]]},
 ]
 
+def _tf_corner(rng):
+    return [{"rng": rng, "seed": 77, "offset": 5,
+             "calls": [["char", 13 + 262144 * 16 + 5, [], 3], ["normal", 3 + 262144 * 4 + 1, [0.0, 1.0], 1],
+                       ["uniform_double", 1 + 262144 * 2 + 1, [], 1]]}]
+
+
+_SO = [(1234, 0), (0xdeadbeefcafe, 12345)]
+
 CASES = {
     "philox": pseudo_cases(404, [(1234, 0), (0xdeadbeef, 12345), (0xAAAAAAAAAAA, 2**40 + 3)],
                            _STRIDE_CORNER),
+    "threefry2x32": pseudo_cases(408, _SO, _tf_corner(408)),
+    "threefry2x64": pseudo_cases(409, _SO, _tf_corner(409)),
+    "threefry4x32": pseudo_cases(410, _SO, _tf_corner(410)),
+    "threefry4x64": pseudo_cases(411, _SO, _tf_corner(411)),
 }

@@ -34,8 +34,10 @@ def torch_dtype(dist):
 
 
 def device_generate(lib, g, dist, n, params=(), mis=0):
-    """One generate call into device memory placed (mis * itemsize) bytes past a 256-byte
-    boundary; returns (status, numpy values)."""
+    """One generate call into device memory placed (mis * itemsize) bytes past a 512-byte
+    boundary (the caching allocator's alignment), which matches the host placement of the
+    oracle ((mis * itemsize) mod 64 past a 64-byte boundary) for mis * itemsize < 64;
+    returns (status, numpy values)."""
     import torch
     suffix, dt, _ = pyorc.DISTS[dist]
     isz = np.dtype(dt).itemsize
