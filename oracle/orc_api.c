@@ -16,7 +16,11 @@ static int is_supported(int t)
         case ORC_RNG_THREEFRY2_32:
         case ORC_RNG_THREEFRY2_64:
         case ORC_RNG_THREEFRY4_32:
-        case ORC_RNG_THREEFRY4_64: return 1;
+        case ORC_RNG_THREEFRY4_64:
+        case ORC_RNG_XORWOW:
+        case ORC_RNG_MRG32K3A:
+        case ORC_RNG_MRG31K3P:
+        case ORC_RNG_LFSR113: return 1;
         default: return 0;
     }
 }
@@ -36,6 +40,14 @@ int orc_create(orc_gen** out, int rng_type)
         return ORC_INTERNAL_ERROR;
     g->rng_type = rng_type;
     g->dims     = 1;
+    if(rng_type == ORC_RNG_LFSR113)
+    {
+        /* default seed {2, 8, 16, 128} (lfsr113.hpp:178-186) */
+        g->seed4[0] = 2;
+        g->seed4[1] = 8;
+        g->seed4[2] = 16;
+        g->seed4[3] = 128;
+    }
     switch(rng_type)
     {
         case ORC_RNG_SOBOL32:
@@ -53,6 +65,7 @@ int orc_destroy(orc_gen* g)
     if(g)
     {
         orc_poisson_free(&g->poisson);
+        free(g->stf.engines);
         free(g);
     }
     return ORC_SUCCESS;
@@ -71,6 +84,16 @@ int orc_initialize(orc_gen* g)
         case ORC_RNG_THREEFRY2_64: orc_threefry_seed(&g->st.threefry, 2, 64, g->seed, g->offset); break;
         case ORC_RNG_THREEFRY4_32: orc_threefry_seed(&g->st.threefry, 4, 32, g->seed, g->offset); break;
         case ORC_RNG_THREEFRY4_64: orc_threefry_seed(&g->st.threefry, 4, 64, g->seed, g->offset); break;
+        case ORC_RNG_XORWOW:
+        case ORC_RNG_MRG32K3A:
+        case ORC_RNG_MRG31K3P:
+        case ORC_RNG_LFSR113:
+        {
+            const int st = orc_stateful_init(g);
+            if(st != ORC_SUCCESS)
+                return st;
+            break;
+        }
         default: return ORC_TYPE_ERROR;
     }
     g->initialized = 1;
@@ -81,6 +104,20 @@ int orc_set_seed(orc_gen* g, unsigned long long seed)
 {
     if(!g)
         return ORC_NOT_CREATED;
+    if(g->rng_type == ORC_RNG_LFSR113)
+    {
+        /* lfsr113.hpp:240-255: overlapping 16-bit shifts, minimums on x and y only */
+        g->seed4[0] = (uint32_t)seed;
+        g->seed4[1] = (uint32_t)(seed >> 16);
+        g->seed4[2] = (uint32_t)(seed >> 32);
+        g->seed4[3] = (uint32_t)(seed >> 48);
+        if(g->seed4[0] < 2)
+            g->seed4[0] += 2;
+        if(g->seed4[1] < 8)
+            g->seed4[1] += 8;
+    }
+    else if(g->rng_type == ORC_RNG_MRG32K3A || g->rng_type == ORC_RNG_MRG31K3P)
+        seed = seed == 0 ? 12345ull : seed; /* mrg.hpp:236-240 */
     g->seed        = seed;
     g->initialized = 0;
     return ORC_SUCCESS;
@@ -88,10 +125,17 @@ int orc_set_seed(orc_gen* g, unsigned long long seed)
 
 int orc_set_seed_uint4(orc_gen* g, uint32_t x, uint32_t y, uint32_t z, uint32_t w)
 {
-    (void)x, (void)y, (void)z, (void)w;
     if(!g)
         return ORC_NOT_CREATED;
-    return ORC_TYPE_ERROR;
+    if(g->rng_type != ORC_RNG_LFSR113)
+        return ORC_TYPE_ERROR;
+    /* lfsr113.hpp:257-269 */
+    g->seed4[0]    = x < 2 ? x + 2 : x;
+    g->seed4[1]    = y < 8 ? y + 8 : y;
+    g->seed4[2]    = z < 16 ? z + 16 : z;
+    g->seed4[3]    = w < 128 ? w + 128 : w;
+    g->initialized = 0;
+    return ORC_SUCCESS;
 }
 
 int orc_set_offset(orc_gen* g, unsigned long long offset)
@@ -165,6 +209,10 @@ static int run(orc_gen* g, void* data, size_t n, const orc_dist* din)
         d.mean_d = m;
         d.std_d  = s;
     }
+    if(g->rng_type == ORC_RNG_MRG31K3P)
+        orc_dist_to_mrg(&d, 1);
+    if(g->rng_type == ORC_RNG_MRG32K3A)
+        orc_dist_to_mrg(&d, 2);
     int st = orc_initialize(g);
     if(st != ORC_SUCCESS)
         return st;
@@ -174,7 +222,7 @@ static int run(orc_gen* g, void* data, size_t n, const orc_dist* din)
         return orc_philox_generate(g, data, n, &d);
     if(is_threefry(g->rng_type))
         return orc_threefry_generate(g, data, n, &d);
-    return ORC_TYPE_ERROR;
+    return orc_stateful_generate(g, data, n, &d);
 }
 
 static int run_kind(orc_gen* g, void* data, size_t n, orc_dist_kind k)

@@ -164,6 +164,86 @@ static inline uint32_t mrg_remap(int mrg, uint32_t v)
     return v;
 }
 
+/* MRG normalisation (rocrand_uniform.h:179-219, constants rocrand_mrg31k3p.h:32,
+ * rocrand_mrg32k3a.h:38) and Box-Muller over it (rocrand_normal.h:138-172). */
+static inline double mrg_norm(int mrg)
+{
+    return mrg == 1 ? 4.656612875245796923e-10 : 2.3283065498378288e-10;
+}
+static inline float mrg_f(int mrg, uint32_t v) { return (float)((double)v * mrg_norm(mrg)); }
+static void mrg_box_muller_f(int mrg, uint32_t x, uint32_t y, float r[2])
+{
+    const float u = mrg_f(mrg, x);
+    const float v = mrg_f(mrg, y) * ORC_2PI;
+    const float s = sqrtf(-2.0f * logf(u));
+    r[0]          = sinf(v) * s;
+    r[1]          = cosf(v) * s;
+}
+static void mrg_box_muller_d(int mrg, uint32_t x, uint32_t y, double r[2])
+{
+    const double u = mrg_f(mrg, x);
+    const double v = mrg_f(mrg, y) * 2.0;
+    const double s = sqrt(-2.0 * log(u));
+    r[0]           = sin(v * ORC_PI_DOUBLE) * s;
+    r[1]           = cos(v * ORC_PI_DOUBLE) * s;
+}
+
+static void mrg_apply(const orc_dist* d, const uint32_t* in, void* outv)
+{
+    switch(d->kind)
+    {
+        case D_FLOAT:
+        {
+            float* o = (float*)outv;
+            o[0]     = mrg_f(d->mrg, in[0]);
+            return;
+        }
+        case D_DOUBLE:
+        {
+            double* o = (double*)outv;
+            o[0]      = (double)in[0] * mrg_norm(d->mrg);
+            return;
+        }
+        case D_NORMAL_F:
+        case D_LOGNORMAL_F:
+        {
+            float  r[2];
+            float* o = (float*)outv;
+            mrg_box_muller_f(d->mrg, in[0], in[1], r);
+            for(int k = 0; k < 2; k++)
+            {
+                const float z = d->mean_f + r[k] * d->std_f;
+                o[k]          = d->kind == D_NORMAL_F ? z : expf(z);
+            }
+            return;
+        }
+        case D_NORMAL_D:
+        case D_LOGNORMAL_D:
+        {
+            double  r[2];
+            double* o = (double*)outv;
+            mrg_box_muller_d(d->mrg, in[0], in[1], r);
+            for(int k = 0; k < 2; k++)
+            {
+                const double z = d->mean_d + r[k] * d->std_d;
+                o[k]           = d->kind == D_NORMAL_D ? z : exp(z);
+            }
+            return;
+        }
+        default: break;
+    }
+}
+
+/* Distribution shapes on an MRG engine: double uniform takes 1 input, double normals 2. */
+void orc_dist_to_mrg(orc_dist* d, int mrg)
+{
+    d->mrg = mrg;
+    if(d->kind == D_DOUBLE)
+        d->iw = 1;
+    if(d->kind == D_NORMAL_D || d->kind == D_LOGNORMAL_D)
+        d->iw = 2;
+}
+
 void orc_dist_init(orc_dist* d, orc_dist_kind kind)
 {
     memset(d, 0, sizeof(*d));
@@ -190,8 +270,31 @@ void orc_dist_init(orc_dist* d, orc_dist_kind kind)
     }
 }
 
-void orc_dist_apply(const orc_dist* d, const uint32_t* in, void* outv)
+void orc_dist_apply(const orc_dist* d, const uint32_t* in_raw, void* outv)
 {
+    /* MRG engines: the single-input distributions see the raw output remapped to
+     * [0, 2^32) (uniform.hpp:224-314 via mrg_uniform_distribution_uint); the float/double
+     * uniforms and normals have their own formulas. */
+    uint32_t        remapped[1];
+    const uint32_t* in = in_raw;
+    if(d->mrg)
+    {
+        switch(d->kind)
+        {
+            case D_FLOAT:
+            case D_DOUBLE:
+            case D_NORMAL_F:
+            case D_NORMAL_D:
+            case D_LOGNORMAL_F:
+            case D_LOGNORMAL_D: mrg_apply(d, in_raw, outv); return;
+            case D_POISSON:
+            case D_POISSON_HUGE: break; /* remapped below, in the Poisson cases */
+            default:
+                remapped[0] = mrg_remap(d->mrg, in_raw[0]);
+                in          = remapped;
+                break;
+        }
+    }
     switch(d->kind)
     {
         case D_UINT:

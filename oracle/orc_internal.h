@@ -112,6 +112,7 @@ void orc_dist_init(orc_dist* d, orc_dist_kind kind);
 /* The same distributions over 64-bit engine words (ThreeFry 2x64/4x64): uniform.hpp:119-200,
  * normal.hpp:138-200, log_normal.hpp:138-200; iw/ow are re-set for 64-bit inputs. */
 void orc_dist_to64(orc_dist* d);
+void orc_dist_to_mrg(orc_dist* d, int mrg); /* 1 = MRG31k3p, 2 = MRG32k3a */
 void orc_dist_apply64(const orc_dist* d, const uint64_t* in, void* out);
 void orc_store(const orc_dist* d, void* data, size_t idx, const void* vals, unsigned k);
 
@@ -157,6 +158,16 @@ void orc_threefry_seed(orc_threefry* e, int dim, int bits, unsigned long long se
                        unsigned long long offset);
 int  orc_threefry_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
 
+/* Stateful engines (XORWOW, MRG32k3a, MRG31k3p, LFSR113): 131072 states of 6 words. */
+typedef struct {
+    uint32_t* engines;
+    uint32_t  start;
+} orc_stateful;
+
+struct orc_gen;
+int orc_stateful_init(struct orc_gen* g);
+int orc_stateful_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
+
 struct orc_gen {
     int                rng_type;
     int                order;
@@ -165,6 +176,8 @@ struct orc_gen {
     int                initialized;
     unsigned           dims;
     orc_poisson        poisson;
+    uint32_t           seed4[4]; /* LFSR113 seed */
+    orc_stateful       stf;
     union {
         orc_philox   philox;
         orc_threefry threefry;

@@ -45,6 +45,11 @@ static rocrand_generator_base_type* make_generator(rocrand_rng_type t)
         case ROCRAND_RNG_PSEUDO_THREEFRY2_64_20:
         case ROCRAND_RNG_PSEUDO_THREEFRY4_32_20:
         case ROCRAND_RNG_PSEUDO_THREEFRY4_64_20: return make_threefry(t);
+        case ROCRAND_RNG_PSEUDO_DEFAULT:
+        case ROCRAND_RNG_PSEUDO_XORWOW:
+        case ROCRAND_RNG_PSEUDO_MRG32K3A:
+        case ROCRAND_RNG_PSEUDO_MRG31K3P:
+        case ROCRAND_RNG_PSEUDO_LFSR113: return make_stateful(t);
         default: return nullptr;
     }
 }

@@ -472,6 +472,126 @@ struct FnNormalD1
     }
 };
 
+// ---- MRG functors (uniform.hpp:224-314, normal.hpp:200-270, log_normal.hpp:200-276,
+//      poisson.hpp:416-441): the raw MRG output lies in [1, m1] and is normalised by the
+//      engine's own constants (rocrand_uniform.h:161-219, rocrand_normal.h:138-172). ----
+
+struct Mrg31k3pNorm // rocrand_mrg31k3p.h:32-34
+{
+    static constexpr double kNorm     = 4.656612875245796923e-10;
+    static constexpr double kUintNorm = 2.000000001396983862;
+};
+struct Mrg32k3aNorm // rocrand_mrg32k3a.h:38-39
+{
+    static constexpr double kNorm     = 2.3283065498378288e-10;
+    static constexpr double kUintNorm = 1.000000048661607;
+};
+
+template<class N>
+__device__ __forceinline__ uint32_t mrg_to_u32(uint32_t v) // (v - 1) * UINT_NORM, truncated
+{
+    return __double2uint_rz(__dmul_rn(__uint2double_rn(v - 1u), N::kUintNorm));
+}
+template<class N>
+__device__ __forceinline__ float mrg_to_f32(uint32_t v)
+{
+    return __double2float_rn(__dmul_rn(__uint2double_rn(v), N::kNorm));
+}
+template<class N>
+__device__ __forceinline__ double mrg_to_f64(uint32_t v)
+{
+    return __dmul_rn(__uint2double_rn(v), N::kNorm);
+}
+
+template<class N, class Inner>
+struct FnMrgRemap // uint/uchar/ushort/half/Poisson: remap to [0, 2^32) then the plain functor
+{
+    using T                      = typename Inner::T;
+    static constexpr unsigned iw = 1, ow = Inner::ow;
+    Inner                     inner;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const uint32_t v = mrg_to_u32<N>(in[0]);
+        inner(&v, out);
+    }
+};
+
+template<class N>
+struct FnMrgFloat
+{
+    using T                      = float;
+    static constexpr unsigned iw = 1, ow = 1;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = mrg_to_f32<N>(in[0]);
+    }
+};
+
+template<class N>
+struct FnMrgDouble
+{
+    using T                      = double;
+    static constexpr unsigned iw = 1, ow = 1;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = mrg_to_f64<N>(in[0]);
+    }
+};
+
+template<class N>
+struct FnMrgNormalF // mrg_box_muller (rocrand_normal.h:138-152)
+{
+    using T                      = float;
+    static constexpr unsigned iw = 2, ow = 2;
+    float                     mean, stddev;
+    bool                      log_normal;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const float u = mrg_to_f32<N>(in[0]);
+        const float v = __fmul_rn(mrg_to_f32<N>(in[1]), 6.2831855f);
+        const float s = __fsqrt_rn(__fmul_rn(-2.0f, logf(u)));
+        float       sv, cv;
+        sincosf(v, &sv, &cv);
+        const float a = __fadd_rn(mean, __fmul_rn(__fmul_rn(sv, s), stddev));
+        const float b = __fadd_rn(mean, __fmul_rn(__fmul_rn(cv, s), stddev));
+        out[0]        = log_normal ? expf(a) : a;
+        out[1]        = log_normal ? expf(b) : b;
+    }
+};
+
+template<class N>
+struct FnMrgNormalD // mrg_box_muller_double (rocrand_normal.h:154-172): float uniforms widened
+{
+    using T                      = double;
+    static constexpr unsigned iw = 2, ow = 2;
+    double                    mean, stddev;
+    bool                      log_normal;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        const double u = (double)mrg_to_f32<N>(in[0]);
+        const double v = (double)mrg_to_f32<N>(in[1]) * 2.0;
+        const double s = __dsqrt_rn(__dmul_rn(-2.0, log(u)));
+        double       sv, cv;
+        sincos(__dmul_rn(v, RB_PI_DOUBLE), &sv, &cv);
+        const double a = __dadd_rn(mean, __dmul_rn(__dmul_rn(sv, s), stddev));
+        const double b = __dadd_rn(mean, __dmul_rn(__dmul_rn(cv, s), stddev));
+        out[0]         = log_normal ? exp(a) : a;
+        out[1]         = log_normal ? exp(b) : b;
+    }
+};
+
+template<class N>
+struct FnMrgPoissonHuge
+{
+    using T                      = uint32_t;
+    static constexpr unsigned iw = 1, ow = 1;
+    double                    sqrt_lambda, lambda;
+    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    {
+        out[0] = poisson_huge(mrg_to_u32<N>(in[0]), sqrt_lambda, lambda);
+    }
+};
+
 template<class F>
 struct has_table
 {
@@ -487,14 +607,34 @@ struct has_table<Fn64Poisson>
 {
     static constexpr bool value = true;
 };
+template<class N>
+struct has_table<FnMrgRemap<N, FnPoisson>>
+{
+    static constexpr bool value = true;
+};
 
 // Stages a Poisson alias table into shared memory (all threads of the block take part)
 // and returns a functor reading it there.  smem holds size doubles then size uints.
 template<class F>
-__device__ __forceinline__ F stage_table(const F& f, unsigned char* smem)
+struct table_of
+{
+    __host__ __device__ static F& get(F& f) { return f; }
+    __host__ __device__ static const F& get(const F& f) { return f; }
+};
+template<class N>
+struct table_of<FnMrgRemap<N, FnPoisson>>
+{
+    using W = FnMrgRemap<N, FnPoisson>;
+    __host__ __device__ static FnPoisson& get(W& f) { return f.inner; }
+    __host__ __device__ static const FnPoisson& get(const W& f) { return f.inner; }
+};
+
+template<class F>
+__device__ __forceinline__ F stage_table(const F& fw, unsigned char* smem)
 {
     if constexpr(has_table<F>::value)
     {
+        const auto& f = table_of<F>::get(fw);
         double*   p = reinterpret_cast<double*>(smem);
         uint32_t* a = reinterpret_cast<uint32_t*>(smem + sizeof(double) * f.size);
         for(uint32_t i = threadIdx.x; i < f.size; i += blockDim.x)
@@ -503,14 +643,15 @@ __device__ __forceinline__ F stage_table(const F& f, unsigned char* smem)
             a[i] = f.alias[i];
         }
         __syncthreads();
-        F g     = f;
-        g.prob  = p;
-        g.alias = a;
+        F     g  = fw;
+        auto& gt = table_of<F>::get(g);
+        gt.prob  = p;
+        gt.alias = a;
         return g;
     }
     else
     {
-        return f;
+        return fw;
     }
 }
 
@@ -518,7 +659,7 @@ template<class F>
 inline size_t table_smem_bytes(const F& f)
 {
     if constexpr(has_table<F>::value)
-        return (size_t)f.size * (sizeof(double) + sizeof(uint32_t));
+        return (size_t)table_of<F>::get(f).size * (sizeof(double) + sizeof(uint32_t));
     else
         return 0;
 }
@@ -550,6 +691,34 @@ inline rocrand_status with_functor(Dist d, const DistParams& p, Body&& body)
             if(p.huge)
                 return body(FnPoissonHuge{p.sqrt_lambda, p.lambda});
             return body(FnPoisson{p.prob, p.alias, p.size, p.offset});
+        default: return ROCRAND_STATUS_TYPE_ERROR;
+    }
+}
+
+// Functor selection for the MRG engines (raw output in [1, m1]).
+template<class N, class Body>
+inline rocrand_status with_functor_mrg(Dist d, const DistParams& p, Body&& body)
+{
+    const float mh = __half2float(__ushort_as_half(p.mean_h));
+    const float sh = __half2float(__ushort_as_half(p.std_h));
+    switch(d)
+    {
+        case Dist::U32: return body(FnMrgRemap<N, FnUint>{FnUint{}});
+        case Dist::U8: return body(FnMrgRemap<N, FnUchar>{FnUchar{}});
+        case Dist::U16: return body(FnMrgRemap<N, FnUshort>{FnUshort{}});
+        case Dist::F32: return body(FnMrgFloat<N>{});
+        case Dist::F64: return body(FnMrgDouble<N>{});
+        case Dist::F16: return body(FnMrgRemap<N, FnHalf>{FnHalf{}});
+        case Dist::NORMAL_F32: return body(FnMrgNormalF<N>{p.mean_f, p.std_f, false});
+        case Dist::LOGNORMAL_F32: return body(FnMrgNormalF<N>{p.mean_f, p.std_f, true});
+        case Dist::NORMAL_F64: return body(FnMrgNormalD<N>{p.mean_d, p.std_d, false});
+        case Dist::LOGNORMAL_F64: return body(FnMrgNormalD<N>{p.mean_d, p.std_d, true});
+        case Dist::NORMAL_F16: return body(FnMrgRemap<N, FnNormalH>{FnNormalH{mh, sh}});
+        case Dist::LOGNORMAL_F16: return body(FnMrgRemap<N, FnLogNormalH>{FnLogNormalH{mh, sh}});
+        case Dist::POISSON:
+            if(p.huge)
+                return body(FnMrgPoissonHuge<N>{p.sqrt_lambda, p.lambda});
+            return body(FnMrgRemap<N, FnPoisson>{FnPoisson{p.prob, p.alias, p.size, p.offset}});
         default: return ROCRAND_STATUS_TYPE_ERROR;
     }
 }

@@ -1,0 +1,768 @@
+// stateful.cu -- XORWOW, MRG32k3a, MRG31k3p and LFSR113 generators.
+//
+// Output contract of the reference (xorwow.hpp:63-161, mrg.hpp:66-157, lfsr113.hpp:66-160),
+// all on E = 131072 persistent engines (512 x 256, config_defaults.hpp:33-66):
+//   * engine e starts as Engine(seed, subsequence = e, offset / E + (e < start)) with
+//     start = offset % E (xorwow.hpp:45-61, 295);
+//   * output vector j (ow elements) is the next application of the distribution on engine
+//     (j + start) % E -- i.e. "slot" t = j % E drives engine (t + start) % E and writes
+//     vectors t, t + E, t + 2E, ...;
+//   * with ow > 1, the slot t == vec_n % E then writes the misaligned head, and then the
+//     tail, from the same engine (xorwow.hpp:121-157);
+//   * afterwards start += ceil(n / ow) mod E (xorwow.hpp:385-389).
+//
+// B200 layout: engine states live in HBM as a structure of arrays (word w of engine e at
+// arena[w * E + e]) so every load/store of a warp is coalesced; a thread owns one slot,
+// keeps its engine in registers for the whole call and writes it back only if it advanced.
+// Initialisation is split: the host applies the common offset jump to the seeded state
+// once (two base states: offset/E and offset/E + 1), the device applies each engine's
+// subsequence jump J^e from per-digit tables (jump_tables.hpp), at most 9 matrix-vector
+// products per engine.
+#include "common.hpp"
+#include "dist.cuh"
+#include "generators.hpp"
+#include "jump_tables.hpp"
+#include "launch.cuh"
+#include "poisson.hpp"
+
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+#include <vector>
+
+namespace rb200
+{
+
+constexpr uint32_t kE = kStatefulEngines; // 131072
+
+// ---- engines (device step functions; the state is NW 32-bit words) ----
+
+struct XorwowEngine // rocrand_xorwow.h:165-177
+{
+    static constexpr int kWords = 6; // x[0..4], d
+    static constexpr int kGf2   = 5; // words covered by the jump matrices
+    uint32_t             w[kWords];
+    __device__ __forceinline__ uint32_t next()
+    {
+        const uint32_t t = w[0] ^ (w[0] >> 2);
+        w[0]             = w[1];
+        w[1]             = w[2];
+        w[2]             = w[3];
+        w[3]             = w[4];
+        w[4]             = (w[4] ^ (w[4] << 4)) ^ (t ^ (t << 1));
+        w[5] += 362437u;
+        return w[5] + w[4];
+    }
+};
+
+struct Lfsr113Engine // rocrand_lfsr113.h:146-160
+{
+    static constexpr int kWords = 4;
+    static constexpr int kGf2   = 4;
+    uint32_t             w[kWords];
+    __device__ __forceinline__ uint32_t next()
+    {
+        uint32_t b;
+        b    = ((w[0] << 6) ^ w[0]) >> 13;
+        w[0] = ((w[0] & 4294967294u) << 18) ^ b;
+        b    = ((w[1] << 2) ^ w[1]) >> 27;
+        w[1] = ((w[1] & 4294967288u) << 2) ^ b;
+        b    = ((w[2] << 13) ^ w[2]) >> 21;
+        w[2] = ((w[2] & 4294967280u) << 7) ^ b;
+        b    = ((w[3] << 3) ^ w[3]) >> 12;
+        w[3] = ((w[3] & 4294967168u) << 13) ^ b;
+        return w[0] ^ w[1] ^ w[2] ^ w[3];
+    }
+};
+
+struct Mrg32k3aEngine // rocrand_mrg32k3a.h:160-190: g1[0..2], g2[0..2]
+{
+    static constexpr int      kWords = 6;
+    static constexpr uint64_t kM1 = 4294967087ull, kM2 = 4294944443ull;
+    uint32_t                  w[kWords];
+    __device__ __forceinline__ static uint64_t mod_m1(uint64_t p)
+    {
+        p = 209ull * (p >> 32) + (p & 0xffffffffull);
+        return p >= kM1 ? p - kM1 : p;
+    }
+    __device__ __forceinline__ static uint64_t mod_m2(uint64_t p)
+    {
+        p = 22853ull * (p >> 32) + (p & 0xffffffffull);
+        p = 22853ull * (p >> 32) + (p & 0xffffffffull);
+        return p >= kM2 ? p - kM2 : p;
+    }
+    __device__ __forceinline__ uint32_t next()
+    {
+        const uint32_t p1 = static_cast<uint32_t>(mod_m1(
+            1403580ull * w[1] + 810728ull * static_cast<uint32_t>(static_cast<uint32_t>(kM1) - w[0])));
+        w[0] = w[1];
+        w[1] = w[2];
+        w[2] = p1;
+        const uint32_t p2 = static_cast<uint32_t>(mod_m2(
+            527612ull * w[5] + 1370589ull * static_cast<uint32_t>(static_cast<uint32_t>(kM2) - w[3])));
+        w[3] = w[4];
+        w[4] = w[5];
+        w[5] = p2;
+        return (p1 - p2) + (p1 <= p2 ? static_cast<uint32_t>(kM1) : 0u);
+    }
+};
+
+struct Mrg31k3pEngine // rocrand_mrg31k3p.h:155-185: x1[0..2], x2[0..2]
+{
+    static constexpr int      kWords = 6;
+    static constexpr uint32_t kM1 = 2147483647u, kM2 = 2147462579u;
+    uint32_t                  w[kWords];
+    __device__ __forceinline__ uint32_t next()
+    {
+        uint32_t t = (((w[1] & 511u) << 22) + (w[1] >> 9)) + (((w[2] & 16777215u) << 7) + (w[2] >> 24));
+        t -= (t >= kM1) ? kM1 : 0u;
+        t += w[2];
+        t -= (t >= kM1) ? kM1 : 0u;
+        w[2] = w[1];
+        w[1] = w[0];
+        w[0] = t;
+        t    = (((w[3] & 65535u) << 15) + 21069u * (w[3] >> 16));
+        t -= (t >= kM2) ? kM2 : 0u;
+        t += ((w[5] & 65535u) << 15);
+        t -= (t >= kM2) ? kM2 : 0u;
+        t += 21069u * (w[5] >> 16);
+        t -= (t >= kM2) ? kM2 : 0u;
+        t += w[5];
+        t -= (t >= kM2) ? kM2 : 0u;
+        w[5] = w[4];
+        w[4] = w[3];
+        w[3] = t;
+        return w[0] - w[3] + (w[0] <= w[3] ? kM1 : 0u);
+    }
+};
+
+// ---- initialisation: engine e = J^e * base[e < start] ----
+
+template<int N>
+__device__ __forceinline__ void gf2_apply(const uint32_t* __restrict__ m, uint32_t* x)
+{
+    uint32_t y[N];
+#pragma unroll
+    for(int k = 0; k < N; k++)
+        y[k] = 0;
+#pragma unroll
+    for(int i = 0; i < N; i++)
+    {
+        const uint32_t xi = x[i];
+#pragma unroll 8
+        for(int b = 0; b < 32; b++)
+        {
+            const uint32_t  mask = 0u - ((xi >> b) & 1u);
+            const uint32_t* row  = m + (i * 32 + b) * N;
+#pragma unroll
+            for(int k = 0; k < N; k++)
+                y[k] ^= mask & __ldg(row + k);
+        }
+    }
+#pragma unroll
+    for(int k = 0; k < N; k++)
+        x[k] = y[k];
+}
+
+__device__ __forceinline__ void mod_apply(const uint64_t* __restrict__ a, uint64_t m, uint32_t* x)
+{
+    uint32_t y[3];
+#pragma unroll
+    for(int r = 0; r < 3; r++)
+    {
+        uint64_t s = 0;
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+            s += (__ldg(reinterpret_cast<const unsigned long long*>(a) + r * 3 + c) * x[c]) % m;
+        y[r] = static_cast<uint32_t>(s % m);
+    }
+#pragma unroll
+    for(int r = 0; r < 3; r++)
+        x[r] = y[r];
+}
+
+struct InitArgs
+{
+    uint32_t base[2][6]; // [0]: offset/E, [1]: offset/E + 1 (engines below start)
+    uint32_t start;
+    uint32_t* arena;
+};
+
+// GF(2) engines (XORWOW: 5 jump words + the Weyl counter copied; LFSR113: 4 words).
+template<int NJ, int NW>
+__global__ void __launch_bounds__(kBlock) init_gf2(InitArgs a, const uint32_t* __restrict__ tables)
+{
+    const uint32_t e = blockIdx.x * kBlock + threadIdx.x;
+    if(e >= kE)
+        return;
+    uint32_t x[NW];
+    const int which = e < a.start ? 1 : 0;
+#pragma unroll
+    for(int k = 0; k < NW; k++)
+        x[k] = a.base[which][k];
+    constexpr size_t msize = static_cast<size_t>(NJ) * 32 * NJ;
+    for(int p = 0; p < kJumpDigits; p++)
+    {
+        const uint32_t d = (e >> (2 * p)) & 3u;
+        if(d)
+            gf2_apply<NJ>(tables + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
+    }
+#pragma unroll
+    for(int k = 0; k < NW; k++)
+        a.arena[static_cast<size_t>(k) * kE + e] = x[k];
+}
+
+// MRG engines: two 3-word components modulo m1 and m2.
+__global__ void __launch_bounds__(kBlock)
+    init_mrg(InitArgs a, const uint64_t* __restrict__ tables, uint64_t m1, uint64_t m2)
+{
+    const uint32_t e = blockIdx.x * kBlock + threadIdx.x;
+    if(e >= kE)
+        return;
+    uint32_t  x[6];
+    const int which = e < a.start ? 1 : 0;
+#pragma unroll
+    for(int k = 0; k < 6; k++)
+        x[k] = a.base[which][k];
+    for(int p = 0; p < kJumpDigits; p++)
+    {
+        const uint32_t d = (e >> (2 * p)) & 3u;
+        if(d)
+        {
+            const uint64_t* t = tables + ((static_cast<size_t>(p) * 3 + (d - 1)) * 2) * 9;
+            mod_apply(t, m1, x);
+            mod_apply(t + 9, m2, x + 3);
+        }
+    }
+#pragma unroll
+    for(int k = 0; k < 6; k++)
+        a.arena[static_cast<size_t>(k) * kE + e] = x[k];
+}
+
+// ---- generation ----
+
+struct FillArgs
+{
+    uint32_t*          arena;
+    uint32_t           start;
+    uint32_t           head, tail;
+    unsigned char*     data;
+    unsigned char*     vec;
+    unsigned long long n, vec_n;
+};
+
+template<class T, unsigned N>
+__device__ __forceinline__ void store_small(unsigned char* p, const T (&v)[N])
+{
+    constexpr unsigned VB = sizeof(T) * N;
+    if constexpr(VB == 4)
+    {
+        uint32_t w;
+        memcpy(&w, v, 4);
+        __stcs(reinterpret_cast<unsigned int*>(p), w);
+    }
+    else if constexpr(VB == 8)
+    {
+        uint2 w;
+        memcpy(&w, v, 8);
+        __stcs(reinterpret_cast<uint2*>(p), w);
+    }
+    else
+    {
+        static_assert(VB == 16, "vector size");
+        uint4 w;
+        memcpy(&w, v, 16);
+        __stcs(reinterpret_cast<uint4*>(p), w);
+    }
+}
+
+template<class E, class F>
+__global__ void __launch_bounds__(kBlock) stateful_fill(FillArgs a, F f)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const F g = stage_table(f, smem);
+
+    const uint32_t t = blockIdx.x * kBlock + threadIdx.x; // slot
+    if(t >= kE)
+        return;
+    const bool loops = t < a.vec_n;
+    const bool edges = F::ow > 1 && (a.head > 0 || a.tail > 0) && (a.vec_n % kE) == t;
+    if(!loops && !edges)
+        return;
+    const uint32_t e = (t + a.start) & (kE - 1);
+    E              eng;
+#pragma unroll
+    for(int k = 0; k < E::kWords; k++)
+        eng.w[k] = a.arena[static_cast<size_t>(k) * kE + e];
+
+    using T = typename F::T;
+    constexpr unsigned VB = F::ow * sizeof(T);
+    uint32_t           in[F::iw];
+    T                  out[F::ow];
+    unsigned long long j = t;
+    for(; j < a.vec_n; j += kE)
+    {
+#pragma unroll
+        for(unsigned i = 0; i < F::iw; i++)
+            in[i] = eng.next();
+        g(in, out);
+        store_small(a.vec + j * VB, out);
+    }
+    if(F::ow > 1 && j == a.vec_n)
+    {
+        T* data = reinterpret_cast<T*>(a.data);
+        if(a.head > 0)
+        {
+            for(unsigned i = 0; i < F::iw; i++)
+                in[i] = eng.next();
+            g(in, out);
+            for(unsigned o = 0; o < a.head; o++)
+                data[o] = out[o];
+        }
+        if(a.tail > 0)
+        {
+            for(unsigned i = 0; i < F::iw; i++)
+                in[i] = eng.next();
+            g(in, out);
+            for(unsigned o = 0; o < a.tail; o++)
+                data[a.n - a.tail + o] = out[o];
+        }
+    }
+#pragma unroll
+    for(int k = 0; k < E::kWords; k++)
+        a.arena[static_cast<size_t>(k) * kE + e] = eng.w[k];
+}
+
+// ---------------------------------------------------------------------------------------
+// Host side: seeding, base states and tables.
+
+enum class Family
+{
+    XORWOW,
+    MRG32K3A,
+    MRG31K3P,
+    LFSR113
+};
+
+// Device copies of the per-digit jump tables, one upload per (family, device).
+struct DeviceTables
+{
+    std::mutex                 mu;
+    std::vector<const void*>   ptr = std::vector<const void*>(64, nullptr);
+};
+
+static const void* digit_tables(Family fam)
+{
+    static DeviceTables cache[4];
+    DeviceTables&       c   = cache[static_cast<int>(fam)];
+    const int           dev = device_info().device;
+    std::lock_guard<std::mutex> lock(c.mu);
+    if(c.ptr[dev])
+        return c.ptr[dev];
+    std::vector<uint32_t> t32;
+    std::vector<uint64_t> t64;
+    switch(fam)
+    {
+        case Family::XORWOW: t32 = gf2_digit_tables(gf2_pow2(xorwow_step_matrix(), 67)); break;
+        case Family::LFSR113: t32 = gf2_digit_tables(gf2_pow2(lfsr113_step_matrix(), 55)); break;
+        case Family::MRG32K3A:
+            t64 = mod_digit_tables(mod_pow2(mrg32k3a_step1(), 76), mod_pow2(mrg32k3a_step2(), 76));
+            break;
+        case Family::MRG31K3P:
+            t64 = mod_digit_tables(mod_pow2(mrg31k3p_step1(), 72), mod_pow2(mrg31k3p_step2(), 72));
+            break;
+    }
+    void*        d     = nullptr;
+    const size_t bytes = t32.empty() ? t64.size() * 8 : t32.size() * 4;
+    if(cudaMalloc(&d, bytes) != cudaSuccess)
+        return nullptr;
+    if(cudaMemcpy(d, t32.empty() ? static_cast<const void*>(t64.data()) : t32.data(), bytes,
+                  cudaMemcpyHostToDevice)
+       != cudaSuccess)
+        return nullptr;
+    c.ptr[dev] = d;
+    return d;
+}
+
+// A^(2^k), k = 0..63, of the one-step map (host offset jumps), computed once per family.
+struct PowTables
+{
+    std::vector<Gf2Matrix> gf2;
+    std::vector<ModMatrix> m1, m2;
+};
+
+static const PowTables& pow_tables(Family fam)
+{
+    static PowTables  t[4];
+    static std::once_flag once[4];
+    const int         i = static_cast<int>(fam);
+    std::call_once(once[i], [&] {
+        PowTables& p = t[i];
+        if(fam == Family::XORWOW || fam == Family::LFSR113)
+        {
+            Gf2Matrix a = fam == Family::XORWOW ? xorwow_step_matrix() : lfsr113_step_matrix();
+            for(int k = 0; k < 64; k++)
+            {
+                p.gf2.push_back(a);
+                a = a.then(a);
+            }
+        }
+        else
+        {
+            ModMatrix a1 = fam == Family::MRG32K3A ? mrg32k3a_step1() : mrg31k3p_step1();
+            ModMatrix a2 = fam == Family::MRG32K3A ? mrg32k3a_step2() : mrg31k3p_step2();
+            for(int k = 0; k < 64; k++)
+            {
+                p.m1.push_back(a1);
+                p.m2.push_back(a2);
+                a1 = a1.mul(a1);
+                a2 = a2.mul(a2);
+            }
+        }
+    });
+    return t[i];
+}
+
+// Applies A^steps to a state (the engine's discard(steps)); XORWOW also advances its Weyl
+// counter d by steps * 362437 (rocrand_xorwow.h:134-145).
+static void host_discard(Family fam, uint32_t* s, unsigned long long steps)
+{
+    const PowTables& p = pow_tables(fam);
+    if(fam == Family::XORWOW)
+        s[5] += static_cast<uint32_t>(steps) * 362437u;
+    for(int k = 0; k < 64 && steps; k++, steps >>= 1)
+    {
+        if(!(steps & 1))
+            continue;
+        uint32_t y[6];
+        if(fam == Family::XORWOW || fam == Family::LFSR113)
+        {
+            p.gf2[k].apply(s, y);
+            std::memcpy(s, y, sizeof(uint32_t) * p.gf2[k].words);
+        }
+        else
+        {
+            p.m1[k].apply(s, y);
+            p.m2[k].apply(s + 3, y + 3);
+            std::memcpy(s, y, sizeof(uint32_t) * 6);
+        }
+    }
+}
+
+// MRG32k3a seeding arithmetic, wrap-around included (rocrand_mrg32k3a.h:103-120, 262-300).
+static uint64_t m32_mod_m1(uint64_t p)
+{
+    p = 209ull * (p >> 32) + (p & 0xffffffffull);
+    return p >= 4294967087ull ? p - 4294967087ull : p;
+}
+static uint64_t m32_mod_m2(uint64_t p)
+{
+    p = 22853ull * (p >> 32) + (p & 0xffffffffull);
+    p = 22853ull * (p >> 32) + (p & 0xffffffffull);
+    return p >= 4294944443ull ? p - 4294944443ull : p;
+}
+template<uint64_t (*Mod)(uint64_t)>
+static uint64_t m32_mod_mul(uint32_t i, uint64_t j, uint64_t m)
+{
+    long long hi = i / 131072, lo = i - hi * 131072;
+    long long t1 = static_cast<long long>(Mod(static_cast<uint64_t>(hi) * j) * 131072);
+    long long t2 = static_cast<long long>(Mod(static_cast<uint64_t>(lo) * j));
+    lo           = static_cast<long long>(Mod(static_cast<uint64_t>(t1 + t2)));
+    if(lo < 0)
+        lo += static_cast<long long>(m);
+    return static_cast<uint64_t>(lo);
+}
+
+// Seeded (engine 0, no jump) state of each family.
+static void seeded_state(Family fam, unsigned long long seed, uint4 seed4, uint32_t* s)
+{
+    switch(fam)
+    {
+        case Family::XORWOW:
+        {
+            // rocrand_xorwow.h:100-131
+            s[0] = 123456789u;
+            s[1] = 362436069u;
+            s[2] = 521288629u;
+            s[3] = 88675123u;
+            s[4] = 5783321u;
+            s[5] = 6615241u;
+            const uint32_t s0 = static_cast<uint32_t>(seed) ^ 0x2c7f967fu;
+            const uint32_t s1 = static_cast<uint32_t>(seed >> 32) ^ 0xa03697cbu;
+            const uint32_t t0 = 1228688033u * s0;
+            const uint32_t t1 = 2073658381u * s1;
+            s[0] += t0;
+            s[1] ^= t0;
+            s[2] += t1;
+            s[3] ^= t1;
+            s[4] += t0;
+            s[5] += t1 + t0;
+            break;
+        }
+        case Family::MRG32K3A:
+        {
+            if(seed == 0)
+                seed = 12345ull;
+            const uint32_t x = static_cast<uint32_t>(seed) ^ 0x55555555u;
+            const uint32_t y = static_cast<uint32_t>((seed >> 32) ^ 0xAAAAAAAAull);
+            s[0]             = static_cast<uint32_t>(m32_mod_mul<m32_mod_m1>(x, seed, 4294967087ull));
+            s[1]             = static_cast<uint32_t>(m32_mod_mul<m32_mod_m1>(y, seed, 4294967087ull));
+            s[2]             = static_cast<uint32_t>(m32_mod_mul<m32_mod_m1>(x, seed, 4294967087ull));
+            s[3]             = static_cast<uint32_t>(m32_mod_mul<m32_mod_m2>(y, seed, 4294944443ull));
+            s[4]             = static_cast<uint32_t>(m32_mod_mul<m32_mod_m2>(x, seed, 4294944443ull));
+            s[5]             = static_cast<uint32_t>(m32_mod_mul<m32_mod_m2>(y, seed, 4294944443ull));
+            break;
+        }
+        case Family::MRG31K3P:
+        {
+            // rocrand_mrg31k3p.h:99-116: (i * j) mod m with the 64-bit product wrapping
+            if(seed == 0)
+                seed = 12345ull;
+            const uint32_t x = static_cast<uint32_t>(seed ^ 0x55555555u);
+            const uint32_t y = static_cast<uint32_t>((seed >> 32) ^ 0xAAAAAAAAu);
+            s[0]             = static_cast<uint32_t>((x * seed) % 2147483647ull);
+            s[1]             = static_cast<uint32_t>((y * seed) % 2147483647ull);
+            s[2]             = static_cast<uint32_t>((x * seed) % 2147483647ull);
+            s[3]             = static_cast<uint32_t>((y * seed) % 2147462579ull);
+            s[4]             = static_cast<uint32_t>((x * seed) % 2147462579ull);
+            s[5]             = static_cast<uint32_t>((y * seed) % 2147462579ull);
+            break;
+        }
+        case Family::LFSR113:
+            s[0] = seed4.x;
+            s[1] = seed4.y;
+            s[2] = seed4.z;
+            s[3] = seed4.w;
+            s[4] = s[5] = 0;
+            break;
+    }
+}
+
+template<Family kFam>
+class StatefulGenerator final : public PseudoGeneratorBase
+{
+public:
+    StatefulGenerator()
+    {
+        if constexpr(kFam == Family::LFSR113)
+            m_seed4 = make_uint4(2u, 8u, 16u, 128u); // lfsr113.hpp:178-186
+    }
+    ~StatefulGenerator() override { cudaFree(m_arena); }
+
+    rocrand_rng_type type() const override
+    {
+        switch(kFam)
+        {
+            case Family::XORWOW: return ROCRAND_RNG_PSEUDO_XORWOW;
+            case Family::MRG32K3A: return ROCRAND_RNG_PSEUDO_MRG32K3A;
+            case Family::MRG31K3P: return ROCRAND_RNG_PSEUDO_MRG31K3P;
+            default: return ROCRAND_RNG_PSEUDO_LFSR113;
+        }
+    }
+
+    rocrand_status set_seed(unsigned long long seed) override
+    {
+        if constexpr(kFam == Family::LFSR113)
+        {
+            // lfsr113.hpp:240-255: 16-bit-overlapping words; only x and y get minimums
+            uint4 s = make_uint4(static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 16),
+                                 static_cast<uint32_t>(seed >> 32), static_cast<uint32_t>(seed >> 48));
+            if(s.x < 2u)
+                s.x += 2u;
+            if(s.y < 8u)
+                s.y += 8u;
+            m_seed4 = s;
+        }
+        else if constexpr(kFam == Family::MRG32K3A || kFam == Family::MRG31K3P)
+        {
+            m_seed = seed == 0 ? 12345ull : seed; // mrg.hpp:236-240
+        }
+        else
+        {
+            m_seed = seed;
+        }
+        m_initialized = false;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    rocrand_status set_seed_uint4(uint4 seed) override
+    {
+        if constexpr(kFam == Family::LFSR113)
+        {
+            // lfsr113.hpp:257-269
+            if(seed.x < 2u)
+                seed.x += 2u;
+            if(seed.y < 8u)
+                seed.y += 8u;
+            if(seed.z < 16u)
+                seed.z += 16u;
+            if(seed.w < 128u)
+                seed.w += 128u;
+            m_seed4       = seed;
+            m_initialized = false;
+            return ROCRAND_STATUS_SUCCESS;
+        }
+        else
+        {
+            (void)seed;
+            return ROCRAND_STATUS_TYPE_ERROR;
+        }
+    }
+
+    rocrand_status set_order(rocrand_ordering order) override
+    {
+        switch(order)
+        {
+            case ROCRAND_ORDERING_PSEUDO_SEEDED:
+                if(kFam != Family::XORWOW)
+                    return ROCRAND_STATUS_OUT_OF_RANGE; // only xorwow.hpp:254-258 lists it
+                [[fallthrough]];
+            case ROCRAND_ORDERING_PSEUDO_DEFAULT:
+            case ROCRAND_ORDERING_PSEUDO_DYNAMIC:
+            case ROCRAND_ORDERING_PSEUDO_BEST:
+            case ROCRAND_ORDERING_PSEUDO_LEGACY:
+                m_order       = order;
+                m_initialized = false;
+                return ROCRAND_STATUS_SUCCESS;
+            default: return ROCRAND_STATUS_OUT_OF_RANGE;
+        }
+    }
+
+    rocrand_status init() override
+    {
+        if(m_initialized)
+            return ROCRAND_STATUS_SUCCESS;
+        if(m_arena == nullptr)
+        {
+            if(cudaMalloc(&m_arena, sizeof(uint32_t) * 6 * kE) != cudaSuccess)
+            {
+                m_arena = nullptr;
+                return ROCRAND_STATUS_ALLOCATION_FAILED;
+            }
+        }
+        m_start = static_cast<uint32_t>(m_offset % kE);
+        unsigned long long jump = m_offset / kE;
+        if constexpr(kFam == Family::LFSR113)
+            jump = static_cast<uint32_t>(jump); // init_lfsr113_engines takes a 32-bit offset
+        InitArgs a{};
+        a.start = m_start;
+        a.arena = m_arena;
+        seeded_state(kFam, m_seed, m_seed4, a.base[0]);
+        host_discard(kFam, a.base[0], jump);
+        std::memcpy(a.base[1], a.base[0], sizeof(a.base[0]));
+        if constexpr(kFam == Family::LFSR113)
+        {
+            // engines below start skip (uint32)(offset/E) + 1, computed in 32 bits
+            seeded_state(kFam, m_seed, m_seed4, a.base[1]);
+            host_discard(kFam, a.base[1], static_cast<uint32_t>(static_cast<uint32_t>(jump) + 1u));
+        }
+        else
+        {
+            host_discard(kFam, a.base[1], 1);
+        }
+        const void* tables = digit_tables(kFam);
+        if(tables == nullptr)
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        const unsigned blocks = kE / kBlock;
+        if constexpr(kFam == Family::XORWOW)
+            init_gf2<5, 6><<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables));
+        else if constexpr(kFam == Family::LFSR113)
+            init_gf2<4, 4><<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables));
+        else if constexpr(kFam == Family::MRG32K3A)
+            init_mrg<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint64_t*>(tables),
+                                                     4294967087ull, 4294944443ull);
+        else
+            init_mrg<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint64_t*>(tables),
+                                                     2147483647ull, 2147462579ull);
+        const rocrand_status st = launch_status();
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        m_initialized = true;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    rocrand_status generate(void* data, size_t n, Dist d, const DistParams& p) override
+    {
+        if(d == Dist::U64)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        rocrand_status st = init();
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        if(data == nullptr)
+            return ROCRAND_STATUS_SUCCESS;
+        const size_t tsize = dist_elem_size(d);
+        if(reinterpret_cast<uintptr_t>(data) % tsize != 0)
+            return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE;
+        auto body = [&](auto f) -> rocrand_status { return run(f, data, n, tsize); };
+        if constexpr(kFam == Family::MRG32K3A)
+            return with_functor_mrg<Mrg32k3aNorm>(d, p, body);
+        else if constexpr(kFam == Family::MRG31K3P)
+            return with_functor_mrg<Mrg31k3pNorm>(d, p, body);
+        else
+            return with_functor(d, p, body);
+    }
+
+    rocrand_status generate_poisson(unsigned int* data, size_t n, double lambda) override
+    {
+        rocrand_status st = init();
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        DistParams p;
+        st = m_poisson.get(lambda, m_stream, false, p);
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        return generate(data, n, Dist::POISSON, p);
+    }
+
+private:
+    template<class F>
+    rocrand_status run(const F& f, void* data, size_t n, size_t tsize)
+    {
+        constexpr unsigned ow   = F::ow;
+        const uintptr_t    addr = reinterpret_cast<uintptr_t>(data);
+        const size_t       mis  = (ow - addr / tsize % ow) % ow;
+        FillArgs           a;
+        a.arena = m_arena;
+        a.start = m_start;
+        a.head  = static_cast<uint32_t>(n < mis ? n : mis);
+        a.tail  = static_cast<uint32_t>((n - a.head) % ow);
+        a.vec_n = (n - a.head) / ow;
+        a.n     = n;
+        a.data  = static_cast<unsigned char*>(data);
+        a.vec   = a.data + mis * tsize;
+        if(n > 0)
+        {
+            const size_t smem = table_smem_bytes(f);
+            using Eng         = std::conditional_t<
+                kFam == Family::XORWOW, XorwowEngine,
+                std::conditional_t<kFam == Family::LFSR113, Lfsr113Engine,
+                                   std::conditional_t<kFam == Family::MRG32K3A, Mrg32k3aEngine,
+                                                      Mrg31k3pEngine>>>;
+            stateful_fill<Eng, F><<<kE / kBlock, kBlock, smem, m_stream>>>(a, f);
+            const rocrand_status st = launch_status();
+            if(st != ROCRAND_STATUS_SUCCESS)
+                return st;
+        }
+        m_start = static_cast<uint32_t>((m_start + (n + ow - 1) / ow) % kE);
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    uint4     m_seed4 = {0, 0, 0, 0};
+    uint32_t* m_arena = nullptr;
+    uint32_t  m_start = 0;
+};
+
+rocrand_generator_base_type* make_stateful(rocrand_rng_type t)
+{
+    switch(t)
+    {
+        case ROCRAND_RNG_PSEUDO_DEFAULT:
+        case ROCRAND_RNG_PSEUDO_XORWOW: return new StatefulGenerator<Family::XORWOW>();
+        case ROCRAND_RNG_PSEUDO_MRG32K3A: return new StatefulGenerator<Family::MRG32K3A>();
+        case ROCRAND_RNG_PSEUDO_MRG31K3P: return new StatefulGenerator<Family::MRG31K3P>();
+        case ROCRAND_RNG_PSEUDO_LFSR113: return new StatefulGenerator<Family::LFSR113>();
+        default: return nullptr;
+    }
+}
+
+} // namespace rb200

@@ -45,6 +45,17 @@ def _tf_corner(rng):
 
 _SO = [(1234, 0), (0xdeadbeefcafe, 12345)]
 
+# Stateful engines: the head/tail slot is vec_n % 131072; pin a call whose vector count is
+# a multiple of the engine count (the head/tail thread is then slot 0).
+def _st_corner(rng):
+    return [{"rng": rng, "seed": 99, "offset": 131072 * 3 + 17,
+             "calls": [["normal", 1 + 131072 * 2 * 2 + 1, [0.0, 1.0], 1],
+                       ["short", 1 + 131072 * 2 + 1, [], 1], ["char", 3 + 131072 * 4 + 2, [], 1],
+                       ["uniform_double", 5, [], 0]]}]
+
+
+_SO_ST = [(1234, 0), (0xdeadbeefcafe, 123456789)]
+
 CASES = {
     "philox": pseudo_cases(404, [(1234, 0), (0xdeadbeef, 12345), (0xAAAAAAAAAAA, 2**40 + 3)],
                            _STRIDE_CORNER),
@@ -52,4 +63,8 @@ CASES = {
     "threefry2x64": pseudo_cases(409, _SO, _tf_corner(409)),
     "threefry4x32": pseudo_cases(410, _SO, _tf_corner(410)),
     "threefry4x64": pseudo_cases(411, _SO, _tf_corner(411)),
+    "xorwow": pseudo_cases(401, _SO_ST, _st_corner(401)),
+    "mrg32k3a": pseudo_cases(402, _SO_ST + [(0, 7)], _st_corner(402)),
+    "mrg31k3p": pseudo_cases(405, _SO_ST, _st_corner(405)),
+    "lfsr113": pseudo_cases(406, _SO_ST, _st_corner(406)),
 }
