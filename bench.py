@@ -36,7 +36,8 @@ SEED = 0xDEADBEEF
 FALLBACK_HBM_GBS = 6650.0
 
 # Generator families in the sweep (rocrand_rng_type values), in the order they were built.
-SWEEP_GENERATORS = [("philox4x32_10", 404)]
+SWEEP_GENERATORS = [("philox4x32_10", 404), ("xorwow", 401), ("mrg32k3a", 402), ("lfsr113", 406),
+                    ("threefry4x32_20", 410)]
 SWEEP_DISTS = [
     ("uint", None), ("uniform", None), ("uniform_double", None), ("uniform_half", None),
     ("normal", (0.0, 1.0)), ("normal_double", (0.0, 1.0)), ("log_normal", (0.0, 1.0)),

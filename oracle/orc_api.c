@@ -20,7 +20,11 @@ static int is_supported(int t)
         case ORC_RNG_XORWOW:
         case ORC_RNG_MRG32K3A:
         case ORC_RNG_MRG31K3P:
-        case ORC_RNG_LFSR113: return 1;
+        case ORC_RNG_LFSR113:
+        case ORC_RNG_SOBOL32:
+        case ORC_RNG_SCRAMBLED_SOBOL32:
+        case ORC_RNG_SOBOL64:
+        case ORC_RNG_SCRAMBLED_SOBOL64: return 1;
         default: return 0;
     }
 }
@@ -94,6 +98,10 @@ int orc_initialize(orc_gen* g)
                 return st;
             break;
         }
+        case ORC_RNG_SOBOL32:
+        case ORC_RNG_SCRAMBLED_SOBOL32:
+        case ORC_RNG_SOBOL64:
+        case ORC_RNG_SCRAMBLED_SOBOL64: g->sobol_offset = (uint32_t)g->offset; break;
         default: return ORC_TYPE_ERROR;
     }
     g->initialized = 1;
@@ -118,6 +126,9 @@ int orc_set_seed(orc_gen* g, unsigned long long seed)
     }
     else if(g->rng_type == ORC_RNG_MRG32K3A || g->rng_type == ORC_RNG_MRG31K3P)
         seed = seed == 0 ? 12345ull : seed; /* mrg.hpp:236-240 */
+    else if(g->rng_type == ORC_RNG_SOBOL32 || g->rng_type == ORC_RNG_SCRAMBLED_SOBOL32
+            || g->rng_type == ORC_RNG_SOBOL64 || g->rng_type == ORC_RNG_SCRAMBLED_SOBOL64)
+        return ORC_SUCCESS; /* quasi-random generators ignore the seed (sobol.hpp:551-554) */
     g->seed        = seed;
     g->initialized = 0;
     return ORC_SUCCESS;
@@ -177,12 +188,24 @@ int orc_set_ordering(orc_gen* g, int order)
     return ORC_SUCCESS;
 }
 
+static int is_sobol(int t)
+{
+    return t == ORC_RNG_SOBOL32 || t == ORC_RNG_SCRAMBLED_SOBOL32 || t == ORC_RNG_SOBOL64
+           || t == ORC_RNG_SCRAMBLED_SOBOL64;
+}
+
+/* sobol.hpp:573-583: 1..20000 dimensions */
 int orc_set_dimensions(orc_gen* g, unsigned int dims)
 {
     if(!g)
         return ORC_NOT_CREATED;
-    (void)dims;
-    return ORC_TYPE_ERROR;
+    if(!is_sobol(g->rng_type))
+        return ORC_TYPE_ERROR;
+    if(dims < 1 || dims > 20000)
+        return ORC_OUT_OF_RANGE;
+    g->dims        = dims;
+    g->initialized = 0;
+    return ORC_SUCCESS;
 }
 
 /* ---- generate dispatch ---- */
@@ -196,6 +219,20 @@ static int is_threefry(int t)
 static int run(orc_gen* g, void* data, size_t n, const orc_dist* din)
 {
     orc_dist d = *din;
+    if(is_sobol(g->rng_type))
+    {
+        /* sobol.hpp:618-640 */
+        if(d.kind == D_ULL && (g->rng_type == ORC_RNG_SOBOL32 || g->rng_type == ORC_RNG_SCRAMBLED_SOBOL32))
+            return ORC_TYPE_ERROR;
+        if(n % g->dims != 0)
+            return ORC_LENGTH_NOT_MULTIPLE;
+        const int st = orc_initialize(g);
+        if(st != ORC_SUCCESS)
+            return st;
+        if(data == NULL)
+            return ORC_SUCCESS;
+        return orc_sobol_generate(g, data, n, &d);
+    }
     /* 64-bit output only from 64-bit engines (philox4x32_10.hpp:359-375, threefry.hpp:316-321) */
     if(d.kind == D_ULL && !is_threefry64(g->rng_type))
         return ORC_TYPE_ERROR;

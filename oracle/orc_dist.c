@@ -518,14 +518,29 @@ int orc_poisson_get(orc_poisson* pm, double lambda, orc_dist* d)
         pm->cap   = orc_poisson_capacity(4000.0);
         pm->prob  = (double*)calloc(pm->cap, sizeof(double));
         pm->alias = (uint32_t*)calloc(pm->cap, sizeof(uint32_t));
-        if(!pm->prob || !pm->alias)
+        pm->cdf   = (double*)calloc(pm->cap, sizeof(double));
+        if(!pm->prob || !pm->alias || !pm->cdf)
             return ORC_ALLOCATION_FAILED;
     }
     unsigned offset = 0;
     unsigned size   = 0;
     if(lambda != pm->lambda)
     {
-        size       = orc_poisson_table(lambda, pm->prob, pm->alias, &offset);
+        size = orc_poisson_table(lambda, pm->prob, pm->alias, &offset);
+        /* the CDF form (discrete.hpp:275-286) of the same normalised probabilities */
+        double* p = (double*)calloc(orc_poisson_capacity(lambda), sizeof(double));
+        unsigned off2;
+        const unsigned sz2 = poisson_probabilities(lambda, p, &off2);
+        double   sum = 0.0;
+        for(unsigned i = 0; i < sz2; i++)
+            sum += p[i];
+        double acc = 0.0;
+        for(unsigned i = 0; i < sz2; i++)
+        {
+            acc += p[i] / sum;
+            pm->cdf[i] = acc;
+        }
+        free(p);
         pm->lambda = lambda;
     }
     else
@@ -537,6 +552,7 @@ int orc_poisson_get(orc_poisson* pm, double lambda, orc_dist* d)
     orc_dist_init(d, D_POISSON);
     d->prob   = pm->prob;
     d->alias  = pm->alias;
+    d->cdf    = pm->cdf;
     d->size   = size;
     d->offset = offset;
     return ORC_SUCCESS;
@@ -546,6 +562,7 @@ void orc_poisson_free(orc_poisson* pm)
 {
     free(pm->prob);
     free(pm->alias);
+    free(pm->cdf);
     memset(pm, 0, sizeof(*pm));
 }
 

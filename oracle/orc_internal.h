@@ -100,6 +100,7 @@ typedef struct orc_dist {
     /* Poisson */
     const double*   prob;
     const uint32_t* alias;
+    const double*   cdf;
     unsigned        size, offset;
     double          lambda, sqrt_lambda;
     /* MRG engines remap raw output before the distribution (see orc_mrg.c) */
@@ -121,6 +122,7 @@ typedef struct {
     double    lambda; /* last lambda whose table is resident, 0 = none */
     double*   prob;
     uint32_t* alias;
+    double*   cdf;
     unsigned  cap;
 } orc_poisson;
 
@@ -167,6 +169,7 @@ typedef struct {
 struct orc_gen;
 int orc_stateful_init(struct orc_gen* g);
 int orc_stateful_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
+int orc_sobol_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
 
 struct orc_gen {
     int                rng_type;
@@ -177,6 +180,7 @@ struct orc_gen {
     unsigned           dims;
     orc_poisson        poisson;
     uint32_t           seed4[4]; /* LFSR113 seed */
+    uint32_t           sobol_offset; /* 32-bit point counter of the Sobol generators */
     orc_stateful       stf;
     union {
         orc_philox   philox;

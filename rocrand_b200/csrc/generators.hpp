@@ -52,5 +52,6 @@ private:
 // Factories of the other generator families (one translation unit each).
 rocrand_generator_base_type* make_threefry(rocrand_rng_type t);
 rocrand_generator_base_type* make_stateful(rocrand_rng_type t);
+rocrand_generator_base_type* make_sobol(rocrand_rng_type t);
 
 } // namespace rb200

@@ -1,0 +1,454 @@
+// sobol.cu -- Sobol32, scrambled Sobol32, Sobol64 and scrambled Sobol64 quasi-random
+// generators.
+//
+// Output contract of the reference (library/src/rng/sobol.hpp:72-256, 618-717): the output is
+// dimension-major, out[d * N + i] = dist(x_d(offset + i)) with N = n / dims, where x_d(k) is
+// the XOR of the direction vectors of dimension d selected by the bits of the Gray code
+// k ^ (k >> 1) (rocrand_sobol32.h:122-170); the scrambled variants XOR the result with a
+// per-dimension constant which, as the reference's generator is written (sobol.hpp:514),
+// is word d of the scrambled direction-vector table.  The point counter is 32-bit and
+// advances by N per call.
+//
+// B200 kernel: grid.y = dimension (its 32/64 vectors staged in shared memory), each thread
+// produces a run of consecutive points by Gray-code steps (one XOR each) and leaps ahead by a
+// power-of-two stride with two XORs (the leap-frog of rocrand_sobol32.h:140-159), writing
+// 16-byte vectors where the row is aligned.  Distributions are applied in registers.
+#include "common.hpp"
+#include "dist.cuh"
+#include "generators.hpp"
+#include "launch.cuh"
+#include "poisson.hpp"
+#include "sobol_tables.hpp"
+
+#include <algorithm>
+#include <type_traits>
+
+namespace rb200
+{
+
+// ---- distributions over a Sobol value (sobol_*_distribution, uniform.hpp:351-442,
+//      normal.hpp:272-330, log_normal.hpp:296-370, poisson.hpp CDF method) ----
+
+// rocrand_normal.h:174-194 roc_f_erfinv, every step rounded as written.
+__device__ __forceinline__ float erfinv_f(float x)
+{
+    const float sgn = (x < 0.0f) ? -1.0f : 1.0f;
+    x               = __fmul_rn(__fsub_rn(1.0f, x), __fadd_rn(1.0f, x));
+    const float lnx = logf(x);
+    if(isnan(lnx))
+        return 1.0f;
+    if(isinf(lnx))
+        return 0.0f;
+    const float tt1 = __fadd_rn(2.0f / (3.141592653f * 0.147f), __fmul_rn(0.5f, lnx));
+    const float tt2 = __fmul_rn(1.0f / (0.147f), lnx);
+    return sgn * __fsqrt_rn(__fadd_rn(-tt1, __fsqrt_rn(__fsub_rn(__fmul_rn(tt1, tt1), tt2))));
+}
+
+// normal_distribution(unsigned int) (rocrand_normal.h:228-233); a 64-bit value uses its high word.
+__device__ __forceinline__ float sobol_normal_f(uint32_t hi32)
+{
+    const float p = u32_to_f32(hi32);
+    return __fmul_rn(RB_SQRT2, erfinv_f(__fsub_rn(__fmul_rn(2.0f, p), 1.0f)));
+}
+
+template<class W>
+__device__ __forceinline__ uint32_t high32(W x)
+{
+    return static_cast<uint32_t>(x >> (8 * sizeof(W) - 32));
+}
+
+// uniform_distribution_double over a Sobol value: 2^-32 based for 32-bit, 2^-53 for 64-bit.
+template<class W>
+__device__ __forceinline__ double sobol_u_f64(W x)
+{
+    if constexpr(sizeof(W) == 4)
+        return u32_to_f64(x);
+    else
+        return __fma_rn(__ull2double_rn(x >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+}
+
+template<class W>
+__device__ __forceinline__ double sobol_normal_d(W x)
+{
+    const double p = sobol_u_f64(x);
+    return __dmul_rn((double)RB_SQRT2, erfinv_d(__dsub_rn(__dmul_rn(2.0, p), 1.0)));
+}
+
+enum class SobolKind : int
+{
+    UINT,
+    ULL,
+    UCHAR,
+    USHORT,
+    FLOAT,
+    DOUBLE,
+    HALF,
+    NORMAL_F,
+    NORMAL_D,
+    NORMAL_H,
+    LOGNORMAL_F,
+    LOGNORMAL_D,
+    LOGNORMAL_H,
+    POISSON,
+    POISSON_HUGE
+};
+
+template<SobolKind K, class W>
+struct SobolOut;
+template<class W> struct SobolOut<SobolKind::UINT, W> { using T = uint32_t; };
+template<class W> struct SobolOut<SobolKind::ULL, W> { using T = unsigned long long; };
+template<class W> struct SobolOut<SobolKind::UCHAR, W> { using T = uint8_t; };
+template<class W> struct SobolOut<SobolKind::USHORT, W> { using T = uint16_t; };
+template<class W> struct SobolOut<SobolKind::FLOAT, W> { using T = float; };
+template<class W> struct SobolOut<SobolKind::DOUBLE, W> { using T = double; };
+template<class W> struct SobolOut<SobolKind::HALF, W> { using T = __half; };
+template<class W> struct SobolOut<SobolKind::NORMAL_F, W> { using T = float; };
+template<class W> struct SobolOut<SobolKind::NORMAL_D, W> { using T = double; };
+template<class W> struct SobolOut<SobolKind::NORMAL_H, W> { using T = __half; };
+template<class W> struct SobolOut<SobolKind::LOGNORMAL_F, W> { using T = float; };
+template<class W> struct SobolOut<SobolKind::LOGNORMAL_D, W> { using T = double; };
+template<class W> struct SobolOut<SobolKind::LOGNORMAL_H, W> { using T = __half; };
+template<class W> struct SobolOut<SobolKind::POISSON, W> { using T = uint32_t; };
+template<class W> struct SobolOut<SobolKind::POISSON_HUGE, W> { using T = uint32_t; };
+
+struct SobolParams
+{
+    float         mean_f, std_f;
+    double        mean_d, std_d;
+    const double* cdf;
+    uint32_t      size, offset;
+    double        lambda, sqrt_lambda;
+};
+
+template<SobolKind K, class W>
+__device__ __forceinline__ typename SobolOut<K, W>::T sobol_apply(W x, const SobolParams& p,
+                                                                   const double* cdf)
+{
+    constexpr int B = 8 * sizeof(W);
+    if constexpr(K == SobolKind::UINT)
+        return high32(x);
+    else if constexpr(K == SobolKind::ULL)
+        return x;
+    else if constexpr(K == SobolKind::UCHAR)
+        return static_cast<uint8_t>(x >> (B - 8));
+    else if constexpr(K == SobolKind::USHORT)
+        return static_cast<uint16_t>(x >> (B - 16));
+    else if constexpr(K == SobolKind::FLOAT)
+        return u32_to_f32(high32(x));
+    else if constexpr(K == SobolKind::DOUBLE)
+        return sobol_u_f64(x);
+    else if constexpr(K == SobolKind::HALF)
+        return u16_to_f16(static_cast<uint32_t>(x >> (B - 16)) & 0xffffu);
+    else if constexpr(K == SobolKind::NORMAL_F)
+        return __fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x)), p.std_f));
+    else if constexpr(K == SobolKind::LOGNORMAL_F)
+        return expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x)))));
+    else if constexpr(K == SobolKind::NORMAL_D)
+        return __dadd_rn(p.mean_d, __dmul_rn(sobol_normal_d(x), p.std_d));
+    else if constexpr(K == SobolKind::LOGNORMAL_D)
+        return exp(__dadd_rn(p.mean_d, __dmul_rn(p.std_d, sobol_normal_d(x))));
+    else if constexpr(K == SobolKind::NORMAL_H)
+        return __float2half_rn(__fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x)), p.std_f)));
+    else if constexpr(K == SobolKind::LOGNORMAL_H)
+        return __float2half_rn(expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x))))));
+    else if constexpr(K == SobolKind::POISSON)
+    {
+        // discrete_cdf (rocrand_discrete.h:92-115): first entry >= x, capped at the last
+        double xd;
+        if constexpr(sizeof(W) == 4)
+            xd = __dmul_rn(__uint2double_rn(x), RB_2POW32_INV_DOUBLE);
+        else
+            xd = __dmul_rn(__ull2double_rn(x), 5.4210108624275221700372640043497e-20);
+        uint32_t lo = 0, hi = p.size - 1;
+        while(lo != hi)
+        {
+            const uint32_t c = (lo + hi) / 2;
+            if(xd > cdf[c])
+                lo = c + 1;
+            else
+                hi = c;
+        }
+        return p.offset + lo;
+    }
+    else
+    {
+        static_assert(K == SobolKind::POISSON_HUGE, "kind");
+        const double nd = sobol_normal_d(x);
+        return (uint32_t)(long long)round(__dadd_rn(__dmul_rn(p.sqrt_lambda, nd), p.lambda));
+    }
+}
+
+// Index of the rightmost zero bit of x; an all-ones x (the 32-bit point counter at its
+// last value) gives 0, as the reference's device engine does (rocrand_sobol32.h:161-166),
+// which also keeps the table index in range.
+template<class W>
+__device__ __forceinline__ uint32_t rzb(W x)
+{
+    int z;
+    if constexpr(sizeof(W) == 4)
+        z = __ffs(~x);
+    else
+        z = __ffsll(static_cast<long long>(~x));
+    return z ? static_cast<uint32_t>(z - 1) : 0u;
+}
+
+template<class W>
+struct SobolCall
+{
+    const W*           vectors; // dims x B
+    const W*           scramble; // scrambled table, read at flat index dim (nullptr: plain)
+    unsigned char*     data;
+    unsigned long long n;       // points per dimension
+    uint32_t           offset;
+    SobolParams        p;
+};
+
+template<class W, SobolKind K>
+__global__ void __launch_bounds__(kBlock) sobol_fill(SobolCall<W> a)
+{
+    using T                = typename SobolOut<K, W>::T;
+    constexpr int      B   = 8 * sizeof(W);
+    constexpr unsigned PPT = sizeof(T) >= 4 ? 4u : 16u / sizeof(T);
+    // 64-bit index for Sobol64 (its engine counter is 64-bit), 32-bit for Sobol32.
+    using I = W;
+
+    __shared__ W v[B];
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t dim = blockIdx.y;
+    if(threadIdx.x < B)
+        v[threadIdx.x] = a.vectors[static_cast<size_t>(dim) * B + threadIdx.x];
+    const double* cdf = nullptr;
+    if constexpr(K == SobolKind::POISSON)
+    {
+        double* s = reinterpret_cast<double*>(smem);
+        for(uint32_t k = threadIdx.x; k < a.p.size; k += blockDim.x)
+            s[k] = a.p.cdf[k];
+        cdf = s;
+    }
+    __syncthreads();
+
+    const W            c      = a.scramble ? a.scramble[dim] : W(0);
+    T*                 row    = reinterpret_cast<T*>(a.data) + static_cast<size_t>(dim) * a.n;
+    const unsigned long long stride = static_cast<unsigned long long>(PPT) * gridDim.x * kBlock;
+    unsigned long long p      = (static_cast<unsigned long long>(blockIdx.x) * kBlock + threadIdx.x) * PPT;
+    if(p >= a.n)
+        return;
+    const uint32_t     lg     = __ffsll(static_cast<long long>(stride)) - 1; // log2(stride)
+    const bool         vec_ok = (reinterpret_cast<uintptr_t>(row) % (PPT * sizeof(T))) == 0;
+
+    // The engine starts at the 32-bit sum offset + p (sobol.hpp:191-196) and then counts in
+    // its own width.
+    I i = static_cast<I>(static_cast<uint32_t>(a.offset + static_cast<uint32_t>(p)));
+    W x = 0;
+    {
+        const I g = i ^ (i >> 1);
+#pragma unroll
+        for(int b = 0; b < B; b++)
+            if((g >> b) & 1)
+                x ^= v[b];
+    }
+    for(; p < a.n; p += stride)
+    {
+        T out[PPT];
+        W xx = x;
+        I ii = i;
+#pragma unroll
+        for(unsigned k = 0; k < PPT; k++)
+        {
+            out[k] = sobol_apply<K, W>(xx ^ c, a.p, cdf);
+            xx ^= v[rzb(ii)];
+            ii++;
+        }
+        if(vec_ok && p + PPT <= a.n)
+        {
+            constexpr unsigned VB = PPT * sizeof(T);
+            if constexpr(VB == 16)
+            {
+                uint4 w;
+                memcpy(&w, out, 16);
+                __stcs(reinterpret_cast<uint4*>(row + p), w);
+            }
+            else
+            {
+                static_assert(VB == 32, "vector");
+                uint4 w[2];
+                memcpy(w, out, 32);
+                __stcs(reinterpret_cast<uint4*>(row + p), w[0]);
+                __stcs(reinterpret_cast<uint4*>(row + p) + 1, w[1]);
+            }
+        }
+        else
+        {
+            for(unsigned k = 0; k < PPT && p + k < a.n; k++)
+                row[p + k] = out[k];
+        }
+        // leap-frog by the power-of-two stride 2^lg: Gray-code bit lg-1 flips, and the bit of
+        // the lowest zero of i above the low lg bits (rocrand_sobol32.h:140-159)
+        x ^= v[lg - 1];
+        x ^= v[rzb(static_cast<I>(i | static_cast<I>(stride - 1)))];
+        i += static_cast<I>(stride);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+
+template<bool kIs64, bool kScrambled>
+class SobolGenerator final : public rocrand_generator_base_type
+{
+    using W = std::conditional_t<kIs64, unsigned long long, uint32_t>;
+
+public:
+    rocrand_rng_type type() const override
+    {
+        if(kIs64)
+            return kScrambled ? ROCRAND_RNG_QUASI_SCRAMBLED_SOBOL64 : ROCRAND_RNG_QUASI_SOBOL64;
+        return kScrambled ? ROCRAND_RNG_QUASI_SCRAMBLED_SOBOL32 : ROCRAND_RNG_QUASI_SOBOL32;
+    }
+    rocrand_status init() override
+    {
+        if(!m_initialized)
+        {
+            m_current     = static_cast<uint32_t>(m_offset); // 32-bit counter (sobol.hpp:604)
+            m_initialized = true;
+        }
+        return ROCRAND_STATUS_SUCCESS;
+    }
+    rocrand_status set_seed(unsigned long long) override { return ROCRAND_STATUS_SUCCESS; }
+    rocrand_status set_offset(unsigned long long offset) override
+    {
+        m_offset      = offset;
+        m_initialized = false;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+    rocrand_status set_order(rocrand_ordering order) override
+    {
+        if(order != ROCRAND_ORDERING_QUASI_DEFAULT)
+            return ROCRAND_STATUS_OUT_OF_RANGE;
+        m_initialized = false;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+    rocrand_status set_dimensions(unsigned int dims) override
+    {
+        if(dims < 1 || dims > kSobolDims)
+            return ROCRAND_STATUS_OUT_OF_RANGE;
+        m_dims        = dims;
+        m_initialized = false;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    rocrand_status generate(void* data, size_t n, Dist d, const DistParams& dp) override
+    {
+        if(!kIs64 && d == Dist::U64)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        if(n % m_dims != 0)
+            return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE;
+        rocrand_status st = init();
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        if(data == nullptr)
+            return ROCRAND_STATUS_SUCCESS;
+        if(reinterpret_cast<uintptr_t>(data) % dist_elem_size(d) != 0)
+            return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE;
+        SobolParams p{};
+        p.mean_f = dp.mean_f;
+        p.std_f  = dp.std_f;
+        p.mean_d = dp.mean_d;
+        p.std_d  = dp.std_d;
+        if(d == Dist::NORMAL_F16 || d == Dist::LOGNORMAL_F16)
+        {
+            p.mean_f = __half2float(__ushort_as_half(dp.mean_h));
+            p.std_f  = __half2float(__ushort_as_half(dp.std_h));
+        }
+        p.cdf         = dp.cdf;
+        p.size        = dp.size;
+        p.offset      = dp.offset;
+        p.lambda      = dp.lambda;
+        p.sqrt_lambda = dp.sqrt_lambda;
+        switch(d)
+        {
+            case Dist::U32: st = launch<SobolKind::UINT>(data, n, p); break;
+            case Dist::U64: st = launch<SobolKind::ULL>(data, n, p); break;
+            case Dist::U8: st = launch<SobolKind::UCHAR>(data, n, p); break;
+            case Dist::U16: st = launch<SobolKind::USHORT>(data, n, p); break;
+            case Dist::F32: st = launch<SobolKind::FLOAT>(data, n, p); break;
+            case Dist::F64: st = launch<SobolKind::DOUBLE>(data, n, p); break;
+            case Dist::F16: st = launch<SobolKind::HALF>(data, n, p); break;
+            case Dist::NORMAL_F32: st = launch<SobolKind::NORMAL_F>(data, n, p); break;
+            case Dist::NORMAL_F64: st = launch<SobolKind::NORMAL_D>(data, n, p); break;
+            case Dist::NORMAL_F16: st = launch<SobolKind::NORMAL_H>(data, n, p); break;
+            case Dist::LOGNORMAL_F32: st = launch<SobolKind::LOGNORMAL_F>(data, n, p); break;
+            case Dist::LOGNORMAL_F64: st = launch<SobolKind::LOGNORMAL_D>(data, n, p); break;
+            case Dist::LOGNORMAL_F16: st = launch<SobolKind::LOGNORMAL_H>(data, n, p); break;
+            case Dist::POISSON:
+                st = dp.huge ? launch<SobolKind::POISSON_HUGE>(data, n, p)
+                             : launch<SobolKind::POISSON>(data, n, p);
+                break;
+            default: return ROCRAND_STATUS_TYPE_ERROR;
+        }
+        if(st == ROCRAND_STATUS_SUCCESS)
+            m_current += static_cast<uint32_t>(n / m_dims);
+        return st;
+    }
+
+    rocrand_status generate_poisson(unsigned int* data, size_t n, double lambda) override
+    {
+        DistParams p;
+        // The quasi-random generators use the CDF form of the table (sobol.hpp:498-499).
+        const rocrand_status st = m_poisson.get(lambda, m_stream, true, p);
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        return generate(data, n, Dist::POISSON, p);
+    }
+
+private:
+    template<SobolKind K>
+    rocrand_status launch(void* data, size_t n, const SobolParams& p)
+    {
+        using T                = typename SobolOut<K, W>::T;
+        constexpr unsigned PPT = sizeof(T) >= 4 ? 4u : 16u / sizeof(T);
+        const W*           vec = static_cast<const W*>(sobol_device_vectors(kIs64, kScrambled));
+        if(vec == nullptr)
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        const unsigned long long N = n / m_dims;
+        if(N == 0)
+            return ROCRAND_STATUS_SUCCESS;
+        SobolCall<W> a;
+        a.vectors  = vec;
+        a.scramble = kScrambled ? vec : nullptr;
+        a.data     = static_cast<unsigned char*>(data);
+        a.n        = N;
+        a.offset   = m_current;
+        a.p        = p;
+        // power-of-two blocks per dimension, about 16 resident blocks per SM in total
+        const unsigned long long want = (N + kBlock * PPT - 1) / (kBlock * PPT);
+        const unsigned long long cap  = std::max<unsigned long long>(
+            1, static_cast<unsigned long long>(device_info().sm_count) * 16 / m_dims);
+        unsigned long long bx = 1;
+        while(bx * 2 <= std::min(want, cap))
+            bx *= 2;
+        const size_t smem = K == SobolKind::POISSON ? p.size * sizeof(double) : 0;
+        sobol_fill<W, K><<<dim3(static_cast<unsigned>(bx), m_dims), kBlock, smem, m_stream>>>(a);
+        return launch_status();
+    }
+
+    unsigned long long m_offset      = 0;
+    uint32_t           m_current     = 0;
+    unsigned int       m_dims        = 1;
+    bool               m_initialized = false;
+    PoissonCache       m_poisson;
+};
+
+rocrand_generator_base_type* make_sobol(rocrand_rng_type t)
+{
+    switch(t)
+    {
+        case ROCRAND_RNG_QUASI_DEFAULT:
+        case ROCRAND_RNG_QUASI_SOBOL32: return new SobolGenerator<false, false>();
+        case ROCRAND_RNG_QUASI_SCRAMBLED_SOBOL32: return new SobolGenerator<false, true>();
+        case ROCRAND_RNG_QUASI_SOBOL64: return new SobolGenerator<true, false>();
+        case ROCRAND_RNG_QUASI_SCRAMBLED_SOBOL64: return new SobolGenerator<true, true>();
+        default: return nullptr;
+    }
+}
+
+} // namespace rb200

@@ -56,6 +56,19 @@ def _st_corner(rng):
 
 _SO_ST = [(1234, 0), (0xdeadbeefcafe, 123456789)]
 
+
+def quasi_cases(rng):
+    """Sobol: dimension-major output, n a multiple of dims; a non-multiple call pins the
+    LENGTH_NOT_MULTIPLE status."""
+    out = []
+    for dims, offset in ((1, 0), (64, 4096), (3, 77)):
+        for dist, params in PSEUDO_DISTS:
+            out.append({"rng": rng, "seed": None, "offset": offset, "dims": dims,
+                        "calls": [[dist, dims * 1000, params, 0], [dist, dims * 37, params, 1],
+                                  [dist, dims * 4099, params, 3], [dist, dims * 2 + 1, params, 0],
+                                  [dist, dims * 257, params, 5]]})
+    return out
+
 CASES = {
     "philox": pseudo_cases(404, [(1234, 0), (0xdeadbeef, 12345), (0xAAAAAAAAAAA, 2**40 + 3)],
                            _STRIDE_CORNER),
@@ -67,4 +80,8 @@ CASES = {
     "mrg32k3a": pseudo_cases(402, _SO_ST + [(0, 7)], _st_corner(402)),
     "mrg31k3p": pseudo_cases(405, _SO_ST, _st_corner(405)),
     "lfsr113": pseudo_cases(406, _SO_ST, _st_corner(406)),
+    "sobol32": quasi_cases(501),
+    "scrambled_sobol32": quasi_cases(502),
+    "sobol64": quasi_cases(504),
+    "scrambled_sobol64": quasi_cases(505),
 }

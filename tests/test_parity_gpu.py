@@ -32,7 +32,10 @@ def _fixture(name):
         return json.load(f)
 
 
-@pytest.mark.parametrize("name", sorted(PSEUDO))
+QUASI = {"sobol32": 501, "scrambled_sobol32": 502, "sobol64": 504, "scrambled_sobol64": 505}
+
+
+@pytest.mark.parametrize("name", sorted(PSEUDO) + sorted(QUASI))
 def test_golden_replay(lib, orc, name):
     for case in _fixture(name):
         g = gu.create(lib, case["rng"], case.get("seed"), case.get("offset"), case.get("dims"))
@@ -112,4 +115,50 @@ def test_full_size_against_oracle_and_continuity(lib, orc, name, dist):
     cat = np.concatenate(got)
     assert np.array_equal(cat.view(np.uint8), big.view(np.uint8))
     del big, cat, got
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("name", sorted(QUASI))
+@pytest.mark.parametrize("dist,params", DISTS, ids=lambda x: str(x))
+def test_quasi_random_sequences(lib, orc, name, dist, params):
+    import zlib
+    rng = np.random.default_rng(zlib.crc32(repr((name, dist, params)).encode()))
+    dims = int(rng.choice([1, 7, 64]))
+    offset = int(rng.integers(0, 2**20))
+    calls = [(dist, dims * n, params, int(rng.integers(0, 16)))
+             for n in ((1 << 18) + 3, 5, int(rng.integers(1, 20000)))]
+    g = gu.create(lib, QUASI[name], None, offset, dims)
+    ref = pyorc.run_sequence(orc, QUASI[name], None, offset, calls, dims=dims)
+    is32 = name in ("sobol32", "scrambled_sobol32")
+    expect_status = 103 if (dist == "ulonglong" and is32) else 0
+    worst = 0
+    try:
+        for (d, n, p, mis), (ost, ovals) in zip(calls, ref):
+            st, vals = gu.device_generate(lib, g, d, n, p, mis)
+            assert st == ost == expect_status
+            if st == 0:
+                worst = max(worst, gu.compare(d, vals, ovals, p))
+    finally:
+        lib.rocrand_destroy_generator(g)
+    print("%s %s dims=%d max ulp %d" % (name, dist, dims, worst))
+
+
+@pytest.mark.parametrize("name,dims", [("sobol32", 1), ("sobol32", 64), ("sobol32", 1000),
+                                       ("scrambled_sobol64", 1), ("scrambled_sobol64", 64),
+                                       ("scrambled_sobol64", 1000)])
+@pytest.mark.parametrize("dist", ["uniform_double", "normal"])
+def test_quasi_config_sizes(lib, orc, name, dims, dist):
+    """The quasi-random workload: 2^20 points per dimension at offset 4096, dimension-major,
+    compared with the oracle in full."""
+    import torch
+    n = dims << 20
+    params = [0.0, 1.0] if dist == "normal" else []
+    g = gu.create(lib, QUASI[name], None, 4096, dims)
+    st, vals = gu.device_generate(lib, g, dist, n, params, 0)
+    lib.rocrand_destroy_generator(g)
+    assert st == 0
+    ost, ovals = pyorc.run_sequence(orc, QUASI[name], None, 4096, [(dist, n, params, 0)], dims=dims)[0]
+    assert ost == 0
+    gu.compare(dist, vals, ovals, params)
+    del vals, ovals
     torch.cuda.empty_cache()
