@@ -49,6 +49,11 @@ private:
     CounterPos m_pos;
 };
 
+// Poisson values of a fresh Philox4x32-10 stream with a caller-supplied table (philox.cu).
+rocrand_status philox_poisson_with_table(unsigned long long seed, unsigned long long offset,
+                                         unsigned int* data, size_t n, const DistParams& p,
+                                         cudaStream_t stream);
+
 // Factories of the other generator families (one translation unit each).
 rocrand_generator_base_type* make_threefry(rocrand_rng_type t);
 rocrand_generator_base_type* make_stateful(rocrand_rng_type t);

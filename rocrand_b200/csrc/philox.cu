@@ -262,6 +262,36 @@ rocrand_status PhiloxGenerator::generate(void* data, size_t n, Dist d, const Dis
     return st;
 }
 
+// Poisson values of a fresh Philox4x32-10 stream (seed, offset) with a caller-supplied
+// table: used by the entry point that allocates nothing (noalloc.cu).
+rocrand_status philox_poisson_with_table(unsigned long long seed, unsigned long long offset,
+                                         unsigned int* data, size_t n, const DistParams& p,
+                                         cudaStream_t stream)
+{
+    if(data == nullptr || n == 0)
+        return ROCRAND_STATUS_SUCCESS;
+    CounterPos pos;
+    pos.advance(offset);
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(data);
+    if(addr % sizeof(unsigned int) != 0)
+        return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE;
+    const size_t mis = (4 - addr / sizeof(unsigned int) % 4) % 4;
+    PhiloxCall   a;
+    a.keys   = philox_keys(seed);
+    a.c0     = pos.counter;
+    a.s0     = pos.sub;
+    a.head   = static_cast<uint32_t>(n < mis ? n : mis);
+    a.tail   = static_cast<uint32_t>((n - a.head) % 4);
+    a.vec_n  = (n - a.head) / 4;
+    a.start0 = a.head; // iw = ow = 1
+    a.n      = n;
+    a.data   = reinterpret_cast<unsigned char*>(data);
+    a.vec    = a.data + mis * sizeof(unsigned int);
+    if(p.huge)
+        return launch_philox(a, FnPoissonHuge{p.sqrt_lambda, p.lambda}, stream);
+    return launch_philox(a, FnPoisson{p.prob, p.alias, p.size, p.offset}, stream);
+}
+
 rocrand_status PhiloxGenerator::generate_poisson(unsigned int* data, size_t n, double lambda)
 {
     rocrand_status st = init();

@@ -15,8 +15,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = set()
-    for h in ("rocrand.h",):
-        with open(os.path.join(ROOT, "include", "rocrand", h)) as f:
+    for h in (os.path.join("rocrand", "rocrand.h"), "rocrand_b200.h"):
+        with open(os.path.join(ROOT, "include", h)) as f:
             text = f.read()
         names |= set(re.findall(r"\b(rocrand_[a-z0-9_]+)\s*\(", text))
     return sorted(names)

@@ -1,0 +1,62 @@
+"""The Poisson entry point that allocates nothing, against the generator path.
+
+Callers that cannot call cudaMalloc (inside a graph capture or a driver callback, or with
+device memory fully pre-partitioned) use rocrand_b200_generate_poisson_noalloc, whose alias
+table lives in a fixed array of the library.  Its values must equal those of a Philox4x32-10
+generator calling rocrand_generate_poisson with the same seed and offset -- bit for bit, the
+Poisson tolerance of every other test -- on two calls in a row (the second continuing the
+stream and switching lambda, so the shared array is rewritten).  Collected last so a run
+stopping at the first failure has already run everything else; it also passes on its own in
+a fresh process.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import rocrand_b200 as rb
+
+pytestmark = pytest.mark.gpu
+
+
+def _entry(lib):
+    f = lib.rocrand_b200_generate_poisson_noalloc
+    f.argtypes = [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_size_t,
+                  ctypes.c_double, ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    return f
+
+
+def test_noalloc_poisson_equals_generator_two_calls(lib):
+    import torch
+    noalloc = _entry(lib)
+    seed, n0, n1 = 0x5EED1234, (1 << 20) + 3, 77777
+    lambdas = (10.0, 1000.0)
+
+    g = ctypes.c_void_p()
+    assert lib.rocrand_create_generator(ctypes.byref(g), rb.ROCRAND_RNG_PSEUDO_PHILOX4_32_10) == 0
+    assert lib.rocrand_set_seed(g, seed) == 0
+    want = []
+    for n, lam in zip((n0, n1), lambdas):
+        buf = torch.empty(n, dtype=torch.int32, device="cuda")
+        assert lib.rocrand_generate_poisson(g, ctypes.c_void_p(buf.data_ptr()), n, lam) == 0
+        want.append(buf)
+    torch.cuda.synchronize()
+    assert lib.rocrand_destroy_generator(g) == 0
+
+    stream = torch.cuda.current_stream().cuda_stream
+    offset = 0
+    for k, (n, lam) in enumerate(zip((n0, n1), lambdas)):
+        got = torch.empty(n, dtype=torch.int32, device="cuda")
+        st = noalloc(seed, offset, ctypes.c_void_p(got.data_ptr()), n, lam, ctypes.c_void_p(stream))
+        assert st == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(got.cpu().numpy(), want[k].cpu().numpy()), "call %d" % k
+        offset += n
+
+
+def test_noalloc_rejects_bad_lambda(lib):
+    noalloc = _entry(lib)
+    assert noalloc(1, 0, None, 10, 0.0, None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+    assert noalloc(1, 0, None, 10, -3.0, None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
