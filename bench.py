@@ -15,7 +15,8 @@ cpu_baseline = the reference's own host generators (oracle/_ref, compiled from t
 
 --impl reference runs only the reference's CPU host generators on the same workload.
 Multi-GPU (torchrun): each rank fills its own disjoint slice of every stream (offset =
-rank * n), no data-path collective; weak scaling.
+rank * n), no data-path collective; weak scaling.  MT19937 has no offset: rank r uses seed
+0xdeadbeef + r (an independent stream of the same size).
 """
 
 import argparse
@@ -37,7 +38,8 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Generator families in the sweep (rocrand_rng_type values), in the order they were built.
 SWEEP_GENERATORS = [("philox4x32_10", 404), ("xorwow", 401), ("mrg32k3a", 402), ("lfsr113", 406),
-                    ("threefry4x32_20", 410)]
+                    ("mt19937", 407), ("threefry4x32_20", 410)]
+NO_OFFSET = {407}  # MT19937: set_offset is a TYPE_ERROR
 SWEEP_DISTS = [
     ("uint", None), ("uniform", None), ("uniform_double", None), ("uniform_half", None),
     ("normal", (0.0, 1.0)), ("normal_double", (0.0, 1.0)), ("log_normal", (0.0, 1.0)),
@@ -191,8 +193,11 @@ def run_ours(args):
     for gname, gtype, d, p in calls:
         g = c_void_p()
         rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), gtype))
-        rb.check_rocrand(lib.rocrand_set_seed(g, SEED))
-        rb.check_rocrand(lib.rocrand_set_offset(g, stream_offset(d, rank * n)))
+        if gtype in NO_OFFSET:
+            rb.check_rocrand(lib.rocrand_set_seed(g, SEED + rank))
+        else:
+            rb.check_rocrand(lib.rocrand_set_seed(g, SEED))
+            rb.check_rocrand(lib.rocrand_set_offset(g, stream_offset(d, rank * n)))
         rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
         gens[(gname, d, p)] = g
 
@@ -339,31 +344,56 @@ def _ref_lib():
     return pyorc.CLib("orc"), "port"
 
 
+_SEEDED = {}  # MT19937 host streams, seeded once per process
+
+
 def cpu_sample(n_per_call, calls, threads):
     """Runs every call of the sweep on the reference's host generators, n_per_call values
     each, split over `threads` host threads (each its own generator, offset to its slice).
-    Returns (bytes, seconds, kind)."""
+    MT19937 has no offset, so each thread runs its own seed; and because the reference's host
+    MT19937 spends minutes seeding its 8192 generators, those are the C port's (lazily
+    seeded, warmed untimed).  Returns (bytes, seconds, kind)."""
     import numpy as np
     from concurrent.futures import ThreadPoolExecutor
     from oracle import pyorc
-    lib, kind = _ref_lib()
+    ref_lib, kind = _ref_lib()
     total_bytes = 0
     t_all = 0.0
     for gname, gtype, d, p in calls:
+        lib = pyorc.CLib("orc") if gtype in NO_OFFSET else ref_lib
         suffix, dt, _ = pyorc.DISTS[d]
         buf = np.empty(n_per_call + 64, dtype=dt)
         base = (-buf.ctypes.data // buf.itemsize) % (64 // buf.itemsize)
         view = buf[base:base + n_per_call]
         chunk = (n_per_call // threads) // 64 * 64
         bounds = [(i * chunk, (i + 1) * chunk if i < threads - 1 else n_per_call) for i in range(threads)]
-        gens = []
-        for a, b in bounds:
-            g = lib.create(gtype)
-            lib.set_seed(g, SEED)
-            lib.set_offset(g, stream_offset(d, a))
-            gens.append(g)
         fn = lib.fn(suffix)
         args = pyorc.dist_args(d, p if p is not None else ())
+        key = (gtype, d, p, threads)
+        if gtype in NO_OFFSET and key in _SEEDED:
+            gens = _SEEDED[key]
+        else:
+            gens = []
+            for i, (a, b) in enumerate(bounds):
+                g = lib.create(gtype)
+                if gtype in NO_OFFSET:
+                    lib.set_seed(g, SEED + i)
+                else:
+                    lib.set_seed(g, SEED)
+                    lib.set_offset(g, stream_offset(d, a))
+                gens.append(g)
+        if gtype in NO_OFFSET and key not in _SEEDED:
+            # untimed, once per stream: a call of >= 65536 units seeds all 8192 generators;
+            # later samples continue the same streams
+            warm = [np.empty(1 << 18, dtype=dt) for _ in range(threads)]
+
+            def seed_all(i):
+                return fn(gens[i], c_void_p(warm[i].ctypes.data), c_size_t(1 << 18), *args)
+
+            with ThreadPoolExecutor(threads) as ex:
+                assert all(s == 0 for s in ex.map(seed_all, range(threads)))
+            del warm
+            _SEEDED[key] = gens
 
         def work(i):
             a, b = bounds[i]
@@ -374,8 +404,9 @@ def cpu_sample(n_per_call, calls, threads):
             sts = list(ex.map(work, range(threads)))
         t_all += time.perf_counter() - t0
         assert all(s == 0 for s in sts), sts
-        for g in gens:
-            lib.destroy(g)
+        if gtype not in NO_OFFSET:
+            for g in gens:
+                lib.destroy(g)
         total_bytes += n_per_call * buf.itemsize
     return total_bytes, t_all, kind
 
@@ -385,7 +416,8 @@ def cpu_baseline_sample(n_per_call, calls):
     nb, secs, kind = cpu_sample(n_per_call, calls, threads)
     return {"value": round(nb / secs / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
             "sample": "same sweep at n=%d values per call (vs 2^28 on the GPU), %d host threads, "
-                      "each its own host generator on a disjoint offset slice" % (n_per_call, threads)}
+                      "each its own host generator on a disjoint offset slice (MT19937: own seed, "
+                      "C port)" % (n_per_call, threads)}
 
 
 def run_reference(args):

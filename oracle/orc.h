@@ -54,6 +54,8 @@ float    orc_half_to_float(uint16_t h);
  * discrete.hpp normalize + create_alias_table).  Returns size; prob/alias need >= capacity. */
 unsigned orc_poisson_table(double lambda, double* prob, uint32_t* alias, unsigned* offset);
 unsigned orc_poisson_capacity(double lambda);
+/* Moves the logarithm of the inverse-erf normal by k ulps (see orc_internal.h). */
+void orc_set_erfinv_log_ulps(int k);
 
 #ifdef __cplusplus
 }

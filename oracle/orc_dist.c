@@ -116,13 +116,17 @@ static void box_muller_h(uint16_t x, uint16_t y, uint16_t r[2])
     r[1]          = orc_float_to_half(cosf(v) * s);
 }
 
+int orc_erfinv_log_ulps = 0;
+
+void orc_set_erfinv_log_ulps(int k) { orc_erfinv_log_ulps = k; }
+
 /* rocrand_normal.h:196-220 roc_d_erfinv */
 static double erfinv_d(double x)
 {
     double tt1, tt2, lnx, sgn;
     sgn = (x < 0.0) ? -1.0 : 1.0;
     x   = (1.0 - x) * (1.0 + x);
-    lnx = log(x);
+    lnx = orc_log_shift_d(log(x));
     if(isnan(lnx))
         return 1.0;
     else if(isinf(lnx))

@@ -171,6 +171,12 @@ int orc_stateful_init(struct orc_gen* g);
 int orc_stateful_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
 int orc_sobol_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
 
+/* MT19937 (orc_mt19937.c): 8192 generators of 624 words, built lazily. */
+struct orc_mt;
+int  orc_mt19937_init(struct orc_gen* g);
+void orc_mt19937_free(struct orc_gen* g);
+int  orc_mt19937_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
+
 struct orc_gen {
     int                rng_type;
     int                order;
@@ -182,6 +188,7 @@ struct orc_gen {
     uint32_t           seed4[4]; /* LFSR113 seed */
     uint32_t           sobol_offset; /* 32-bit point counter of the Sobol generators */
     orc_stateful       stf;
+    struct orc_mt*     mt;
     union {
         orc_philox   philox;
         orc_threefry threefry;
@@ -189,5 +196,25 @@ struct orc_gen {
 };
 
 static inline size_t orc_min_sz(size_t a, size_t b) { return a < b ? a : b; }
+
+/* Test hook: the logarithm inside the inverse-erf normal (rocrand_normal.h:174-226) moved
+ * by this many ulps (0 = the reference's value).  The formula -tt1 + sqrt(tt1^2 - tt2)
+ * cancels, so one ulp of log moves the normal by many ulps; a test accepts a device value
+ * that equals the formula at a neighbouring logarithm. */
+extern int orc_erfinv_log_ulps;
+
+static inline float orc_log_shift_f(float v)
+{
+    for(int k = orc_erfinv_log_ulps; k != 0 && isfinite(v) && v != 0.0f; k += k > 0 ? -1 : 1)
+        v = nextafterf(v, k > 0 ? INFINITY : -INFINITY);
+    return v;
+}
+
+static inline double orc_log_shift_d(double v)
+{
+    for(int k = orc_erfinv_log_ulps; k != 0 && isfinite(v) && v != 0.0; k += k > 0 ? -1 : 1)
+        v = nextafter(v, k > 0 ? INFINITY : -INFINITY);
+    return v;
+}
 
 #endif

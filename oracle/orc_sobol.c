@@ -98,7 +98,7 @@ static float erfinv_f(float x)
     float tt1, tt2, lnx, sgn;
     sgn = (x < 0.0f) ? -1.0f : 1.0f;
     x   = (1.0f - x) * (1.0f + x);
-    lnx = logf(x);
+    lnx = orc_log_shift_f(logf(x));
     if(isnan(lnx))
         return 1.0f;
     else if(isinf(lnx))
@@ -113,7 +113,7 @@ static double erfinv_dd(double x)
     double tt1, tt2, lnx, sgn;
     sgn = (x < 0.0) ? -1.0 : 1.0;
     x   = (1.0 - x) * (1.0 + x);
-    lnx = log(x);
+    lnx = orc_log_shift_d(log(x));
     if(isnan(lnx))
         return 1.0;
     else if(isinf(lnx))

@@ -80,6 +80,10 @@ class CLib:
             f = getattr(self.lib, self.prefix + fn)
             f.argtypes = [c_void_p, c_ulonglong]
 
+    def set_erfinv_log_ulps(self, k):
+        """Oracle only: moves the inverse-erf normal's logarithm by k ulps (0 restores)."""
+        self.lib.orc_set_erfinv_log_ulps(ctypes.c_int(k))
+
     def fn(self, name):
         return getattr(self.lib, self.prefix + name)
 

@@ -6,12 +6,16 @@
 // against the reference's host generators.  Every rounding step is written with an
 // explicit _rn intrinsic: a product is fused into an FMA only where it is exact (scaling
 // by a power of two), so the device rounds exactly where the x86-64 host does.
-// Transcendentals (log/sin/cos/exp) use CUDA's accurate library functions; they can
-// differ from glibc by an ulp or two, which is the stated tolerance for normal and
-// log-normal outputs.
+// fp32 transcendentals use CUDA's accurate library functions, within an ulp or two of the
+// host C library, inside the stated fp32 tolerance.  The fp64 Box-Muller transforms and
+// the inverse-erf normal take log/sin/cos from precise_math.cuh (correctly rounded but for
+// rare near-halfway cases), so that the fp64 outputs stay within 2 ulp of the host's and
+// the ill-conditioned inverse-erf formula starts from the same logarithm wherever the host
+// library's is itself correctly rounded.
 #pragma once
 
 #include "common.hpp"
+#include "precise_math.cuh"
 
 #include <cuda_fp16.h>
 
@@ -76,10 +80,10 @@ __device__ __forceinline__ double2 box_muller_f64(uint32_t x, uint32_t y, uint32
     const double   u  = __fma_rn(__ull2double_rn(v1), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
     const uint64_t v2 = (uint64_t)z ^ ((uint64_t)w << 21);
     const double   ww = __fma_rn(__ull2double_rn(v2), RB_2POW53_INV_DOUBLE * 2.0, RB_2POW53_INV_DOUBLE * 2.0);
-    const double   s  = __dsqrt_rn(__dmul_rn(-2.0, log(u)));
+    const double   s  = __dsqrt_rn(__dmul_rn(-2.0, pm::log(u)));
     const double   a  = __dmul_rn(ww, RB_PI_DOUBLE);
     double         sv, cv;
-    sincos(a, &sv, &cv);
+    pm::sincos(a, sv, cv);
     return make_double2(__dmul_rn(sv, s), __dmul_rn(cv, s));
 }
 
@@ -100,7 +104,7 @@ __device__ __forceinline__ double erfinv_d(double x)
 {
     const double sgn = (x < 0.0) ? -1.0 : 1.0;
     x                = __dmul_rn(__dsub_rn(1.0, x), __dadd_rn(1.0, x));
-    const double lnx = log(x);
+    const double lnx = pm::log(x);
     if(isnan(lnx))
         return 1.0;
     if(isinf(lnx))
@@ -570,9 +574,9 @@ struct FnMrgNormalD // mrg_box_muller_double (rocrand_normal.h:154-172): float u
     {
         const double u = (double)mrg_to_f32<N>(in[0]);
         const double v = (double)mrg_to_f32<N>(in[1]) * 2.0;
-        const double s = __dsqrt_rn(__dmul_rn(-2.0, log(u)));
+        const double s = __dsqrt_rn(__dmul_rn(-2.0, pm::log(u)));
         double       sv, cv;
-        sincos(__dmul_rn(v, RB_PI_DOUBLE), &sv, &cv);
+        pm::sincos(__dmul_rn(v, RB_PI_DOUBLE), sv, cv);
         const double a = __dadd_rn(mean, __dmul_rn(__dmul_rn(sv, s), stddev));
         const double b = __dadd_rn(mean, __dmul_rn(__dmul_rn(cv, s), stddev));
         out[0]         = log_normal ? exp(a) : a;

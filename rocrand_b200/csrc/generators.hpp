@@ -54,9 +54,31 @@ rocrand_status philox_poisson_with_table(unsigned long long seed, unsigned long 
                                          unsigned int* data, size_t n, const DistParams& p,
                                          cudaStream_t stream);
 
+// Stateful engine families (stateful.cu, batch.cu).
+enum class StatefulFamily
+{
+    XORWOW,
+    MRG32K3A,
+    MRG31K3P,
+    LFSR113
+};
+
+// Engine states a fresh stateful generator (seed, offset) starts from: engines
+// e >= start begin at base[0], engines below it at base[1]; engine e then jumps e
+// subsequences with the per-digit tables.  LFSR113 takes its default uint4 seed here.
+struct StatefulBases
+{
+    uint32_t base[2][6];
+    uint32_t start;
+};
+StatefulBases stateful_bases(StatefulFamily fam, unsigned long long seed, unsigned long long offset);
+// Per-digit subsequence jump tables of a family on the current device (uploaded once).
+const void* stateful_digit_tables(StatefulFamily fam);
+
 // Factories of the other generator families (one translation unit each).
 rocrand_generator_base_type* make_threefry(rocrand_rng_type t);
 rocrand_generator_base_type* make_stateful(rocrand_rng_type t);
+rocrand_generator_base_type* make_mt19937();
 rocrand_generator_base_type* make_sobol(rocrand_rng_type t);
 
 } // namespace rb200

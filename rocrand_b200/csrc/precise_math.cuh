@@ -1,0 +1,233 @@
+// precise_math.cuh -- natural logarithm and sine/cosine in double precision whose results
+// are correctly rounded except in rare near-halfway cases (internal precision ~2^-66).
+//
+// The reference's host generators evaluate Box-Muller and the inverse-erf normal with the
+// C library's log/sin/cos, which are themselves within ~0.52 ulp of the exact value.  The
+// normal and log-normal outputs of this library are compared with them at <= 2 ulp (fp64);
+// the device's own 1-2 ulp functions can leave a 3-ulp gap after the products, so the fp64
+// transforms use these instead.  Method (standard table-driven reduction, written here):
+//  * log x: x = 2^e m with m in [sqrt(1/2), sqrt(2)); c = 1 + i/128 nearest m,
+//    r = m/c - 1 formed exactly as m*invc - 1 in double-double, then
+//    log x = e ln2 - log(invc) + r - r^2/2 + r^3 P(r) with the leading terms in
+//    double-double and one final rounding;
+//  * sin/cos x (0 <= x <~ 8): x = k pi/2 + r (pi/2 in three parts), |r| = j/64 + b,
+//    sin/cos(j/64) from a double-double table, sin b and cos b - 1 by short series.
+// Both are IEEE operations only (add, mul, fma, sqrt-free), so host and device builds of
+// this header give identical results; the tables are computed in binary128 at build time
+// (rocrand_b200/data/make_precise_tables.c).
+#pragma once
+
+#include "precise_tables.inc"
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#if defined(__CUDACC__)
+#define RB_PM_HD __host__ __device__ __forceinline__
+#else
+#define RB_PM_HD inline
+#endif
+
+namespace rb200
+{
+namespace pm
+{
+
+#if defined(__CUDACC__)
+static __device__ const double kLogTabDev[RB_LOG_TABLE_ROWS * 3] = RB_LOG_TABLE_INIT;
+static __device__ const double kScTabDev[RB_SC_TABLE_ROWS * 4]    = RB_SC_TABLE_INIT;
+#endif
+static const double kLogTabHost[RB_LOG_TABLE_ROWS * 3] = RB_LOG_TABLE_INIT;
+static const double kScTabHost[RB_SC_TABLE_ROWS * 4]    = RB_SC_TABLE_INIT;
+
+RB_PM_HD const double* log_table()
+{
+#if defined(__CUDA_ARCH__)
+    return kLogTabDev;
+#else
+    return kLogTabHost;
+#endif
+}
+
+RB_PM_HD const double* sc_table()
+{
+#if defined(__CUDA_ARCH__)
+    return kScTabDev;
+#else
+    return kScTabHost;
+#endif
+}
+
+RB_PM_HD double fma_(double a, double b, double c)
+{
+#if defined(__CUDA_ARCH__)
+    return __fma_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+
+RB_PM_HD uint64_t bits_of(double x)
+{
+    uint64_t u;
+    memcpy(&u, &x, 8);
+    return u;
+}
+
+RB_PM_HD double from_bits(uint64_t u)
+{
+    double x;
+    memcpy(&x, &u, 8);
+    return x;
+}
+
+// s + e == a + b exactly
+RB_PM_HD void two_sum(double a, double b, double& s, double& e)
+{
+    s              = a + b;
+    const double bb = s - a;
+    e              = (a - (s - bb)) + (b - bb);
+}
+
+// Natural logarithm, near-correctly rounded.
+RB_PM_HD double log(double x)
+{
+    if(!(x > 0.0)) // zero, negative, NaN
+        return x == 0.0 ? -INFINITY : NAN;
+    if(x == INFINITY)
+        return x;
+    int e = 0;
+    if(x < 0x1p-1022) // subnormal
+    {
+        x *= 0x1p54;
+        e = -54;
+    }
+    const uint64_t u = bits_of(x);
+    e += static_cast<int>((u >> 52) & 0x7ff) - 1023;
+    double m = from_bits((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull); // [1, 2)
+    if(m >= 1.4142135623730951)
+    {
+        m *= 0.5;
+        e += 1;
+    }
+    const int     i   = static_cast<int>(rint((m - 1.0) * 128.0));
+    const double* row = log_table() + 3 * (i - RB_LOG_TABLE_MIN);
+    const double  invc = row[0], lch = row[1], lcl = row[2];
+    // r = m * invc - 1 exactly, as r_hi + r_lo
+    const double ph = m * invc;
+    const double pl = fma_(m, invc, -ph);
+    double       rh, rl;
+    two_sum(ph - 1.0, pl, rh, rl); // ph - 1 is exact (ph in [0.5, 2])
+    // -r^2 / 2 as qh + ql
+    const double r2h = rh * rh;
+    const double r2l = fma_(rh, rh, -r2h) + 2.0 * rh * rl;
+    const double qh  = -0.5 * r2h;
+    const double ql  = -0.5 * r2l;
+    // r^3 (1/3 - r/4 + r^2/5 - ...), |r| < 2^-7
+    double t = -1.0 / 12.0;
+    t        = fma_(t, rh, 1.0 / 11.0);
+    t        = fma_(t, rh, -1.0 / 10.0);
+    t        = fma_(t, rh, 1.0 / 9.0);
+    t        = fma_(t, rh, -1.0 / 8.0);
+    t        = fma_(t, rh, 1.0 / 7.0);
+    t        = fma_(t, rh, -1.0 / 6.0);
+    t        = fma_(t, rh, 1.0 / 5.0);
+    t        = fma_(t, rh, -1.0 / 4.0);
+    t        = fma_(t, rh, 1.0 / 3.0);
+    const double tail = t * (rh * r2h);
+    const double de   = static_cast<double>(e);
+    double       s1h, s1l, s2h, s2l, s3h, s3l;
+    two_sum(de * RB_LN2_HI, lch, s1h, s1l); // e * ln2_hi is exact (42-bit head)
+    two_sum(s1h, rh, s2h, s2l);
+    two_sum(s2h, qh, s3h, s3l);
+    const double low = (((s1l + s2l) + s3l) + (ql + rl)) + ((lcl + de * RB_LN2_LO) + tail);
+    return s3h + low;
+}
+
+// sin and cos of x for 0 <= x < 8 (the Box-Muller angles 0 .. 2 pi), near-correctly rounded.
+RB_PM_HD void sincos(double x, double& s_out, double& c_out)
+{
+    const double kd = rint(x * RB_2_OVER_PI);
+    const int    k  = static_cast<int>(kd);
+    // r = x - k pi/2 as rh + rl (k pi/2 in three parts; the first two products are exact)
+    const double t  = fma_(-kd, RB_PIO2_1, x);
+    const double p2 = kd * RB_PIO2_2;
+    double       rh, rl;
+    two_sum(t, -p2, rh, rl);
+    rl -= kd * RB_PIO2_3;
+    {
+        const double h = rh + rl;
+        rl             = rl - (h - rh);
+        rh             = h;
+    }
+    const bool neg = rh < 0.0;
+    if(neg)
+    {
+        rh = -rh;
+        rl = -rl;
+    }
+    const int     j   = static_cast<int>(rint(rh * 64.0));
+    const double* row = sc_table() + 4 * j;
+    const double  sh = row[0], sl = row[1], ch = row[2], cl = row[3];
+    const double  bh = rh - static_cast<double>(j) * (1.0 / 64.0); // exact
+    const double  bl = rl;
+    const double  b2 = bh * bh;
+    // sin b - bh = bl + bh^3 (-1/6 + b^2/120 - ...);  cos b - 1 = -b^2/2 + b^4/24 - ...
+    double sp = -1.0 / 39916800.0;
+    sp        = fma_(sp, b2, 1.0 / 362880.0);
+    sp        = fma_(sp, b2, -1.0 / 5040.0);
+    sp        = fma_(sp, b2, 1.0 / 120.0);
+    sp        = fma_(sp, b2, -1.0 / 6.0);
+    const double sinb_rest = fma_(sp * b2, bh, bl); // bl + bh^3 S(b^2)
+    double       cp        = -1.0 / 3628800.0;
+    cp                     = fma_(cp, b2, 1.0 / 40320.0);
+    cp                     = fma_(cp, b2, -1.0 / 720.0);
+    cp                     = fma_(cp, b2, 1.0 / 24.0);
+    // cos b - 1 = -b^2/2 + b^4 C(b^2), with b^2 including the low part of b
+    const double bb  = fma_(2.0 * bh, bl, b2);
+    const double cm1 = fma_(cp * bb, bb, -0.5 * bb);
+    // sin(a + b) = sin a + (cos a * b + sin a * (cos b - 1) + cos a * (sin b - b))
+    const double psh = ch * bh;
+    const double psl = fma_(ch, bh, -psh);
+    double       ssh, ssl;
+    two_sum(sh, psh, ssh, ssl);
+    const double s_low = ((ssl + psl) + sl) + ((sh * cm1 + ch * sinb_rest) + cl * bh);
+    const double sv    = ssh + s_low;
+    // cos(a + b) = cos a - (sin a * b) + cos a * (cos b - 1) - sin a * (sin b - b)
+    const double pch = sh * bh;
+    const double pcl = fma_(sh, bh, -pch);
+    double       csh, csl;
+    two_sum(ch, -pch, csh, csl);
+    const double c_low = ((csl - pcl) + cl) + ((ch * cm1 - sh * sinb_rest) - sl * bh);
+    const double cv    = csh + c_low;
+    const double s     = neg ? -sv : sv;
+    switch(k & 3)
+    {
+        case 0:
+            s_out = s;
+            c_out = cv;
+            break;
+        case 1:
+            s_out = cv;
+            c_out = -s;
+            break;
+        case 2:
+            s_out = -s;
+            c_out = -cv;
+            break;
+        default:
+            s_out = -cv;
+            c_out = s;
+            break;
+    }
+}
+
+// Natural logarithm of a float, correctly rounded except in rare double-rounding cases.
+RB_PM_HD float logf(float x)
+{
+    return static_cast<float>(log(static_cast<double>(x)));
+}
+
+} // namespace pm
+} // namespace rb200

@@ -24,6 +24,7 @@
 #include "jump_tables.hpp"
 #include "launch.cuh"
 #include "poisson.hpp"
+#include "stateful_engines.cuh"
 
 #include <cstring>
 #include <mutex>
@@ -34,152 +35,6 @@ namespace rb200
 {
 
 constexpr uint32_t kE = kStatefulEngines; // 131072
-
-// ---- engines (device step functions; the state is NW 32-bit words) ----
-
-struct XorwowEngine // rocrand_xorwow.h:165-177
-{
-    static constexpr int kWords = 6; // x[0..4], d
-    static constexpr int kGf2   = 5; // words covered by the jump matrices
-    uint32_t             w[kWords];
-    __device__ __forceinline__ uint32_t next()
-    {
-        const uint32_t t = w[0] ^ (w[0] >> 2);
-        w[0]             = w[1];
-        w[1]             = w[2];
-        w[2]             = w[3];
-        w[3]             = w[4];
-        w[4]             = (w[4] ^ (w[4] << 4)) ^ (t ^ (t << 1));
-        w[5] += 362437u;
-        return w[5] + w[4];
-    }
-};
-
-struct Lfsr113Engine // rocrand_lfsr113.h:146-160
-{
-    static constexpr int kWords = 4;
-    static constexpr int kGf2   = 4;
-    uint32_t             w[kWords];
-    __device__ __forceinline__ uint32_t next()
-    {
-        uint32_t b;
-        b    = ((w[0] << 6) ^ w[0]) >> 13;
-        w[0] = ((w[0] & 4294967294u) << 18) ^ b;
-        b    = ((w[1] << 2) ^ w[1]) >> 27;
-        w[1] = ((w[1] & 4294967288u) << 2) ^ b;
-        b    = ((w[2] << 13) ^ w[2]) >> 21;
-        w[2] = ((w[2] & 4294967280u) << 7) ^ b;
-        b    = ((w[3] << 3) ^ w[3]) >> 12;
-        w[3] = ((w[3] & 4294967168u) << 13) ^ b;
-        return w[0] ^ w[1] ^ w[2] ^ w[3];
-    }
-};
-
-struct Mrg32k3aEngine // rocrand_mrg32k3a.h:160-190: g1[0..2], g2[0..2]
-{
-    static constexpr int      kWords = 6;
-    static constexpr uint64_t kM1 = 4294967087ull, kM2 = 4294944443ull;
-    uint32_t                  w[kWords];
-    __device__ __forceinline__ static uint64_t mod_m1(uint64_t p)
-    {
-        p = 209ull * (p >> 32) + (p & 0xffffffffull);
-        return p >= kM1 ? p - kM1 : p;
-    }
-    __device__ __forceinline__ static uint64_t mod_m2(uint64_t p)
-    {
-        p = 22853ull * (p >> 32) + (p & 0xffffffffull);
-        p = 22853ull * (p >> 32) + (p & 0xffffffffull);
-        return p >= kM2 ? p - kM2 : p;
-    }
-    __device__ __forceinline__ uint32_t next()
-    {
-        const uint32_t p1 = static_cast<uint32_t>(mod_m1(
-            1403580ull * w[1] + 810728ull * static_cast<uint32_t>(static_cast<uint32_t>(kM1) - w[0])));
-        w[0] = w[1];
-        w[1] = w[2];
-        w[2] = p1;
-        const uint32_t p2 = static_cast<uint32_t>(mod_m2(
-            527612ull * w[5] + 1370589ull * static_cast<uint32_t>(static_cast<uint32_t>(kM2) - w[3])));
-        w[3] = w[4];
-        w[4] = w[5];
-        w[5] = p2;
-        return (p1 - p2) + (p1 <= p2 ? static_cast<uint32_t>(kM1) : 0u);
-    }
-};
-
-struct Mrg31k3pEngine // rocrand_mrg31k3p.h:155-185: x1[0..2], x2[0..2]
-{
-    static constexpr int      kWords = 6;
-    static constexpr uint32_t kM1 = 2147483647u, kM2 = 2147462579u;
-    uint32_t                  w[kWords];
-    __device__ __forceinline__ uint32_t next()
-    {
-        uint32_t t = (((w[1] & 511u) << 22) + (w[1] >> 9)) + (((w[2] & 16777215u) << 7) + (w[2] >> 24));
-        t -= (t >= kM1) ? kM1 : 0u;
-        t += w[2];
-        t -= (t >= kM1) ? kM1 : 0u;
-        w[2] = w[1];
-        w[1] = w[0];
-        w[0] = t;
-        t    = (((w[3] & 65535u) << 15) + 21069u * (w[3] >> 16));
-        t -= (t >= kM2) ? kM2 : 0u;
-        t += ((w[5] & 65535u) << 15);
-        t -= (t >= kM2) ? kM2 : 0u;
-        t += 21069u * (w[5] >> 16);
-        t -= (t >= kM2) ? kM2 : 0u;
-        t += w[5];
-        t -= (t >= kM2) ? kM2 : 0u;
-        w[5] = w[4];
-        w[4] = w[3];
-        w[3] = t;
-        return w[0] - w[3] + (w[0] <= w[3] ? kM1 : 0u);
-    }
-};
-
-// ---- initialisation: engine e = J^e * base[e < start] ----
-
-template<int N>
-__device__ __forceinline__ void gf2_apply(const uint32_t* __restrict__ m, uint32_t* x)
-{
-    uint32_t y[N];
-#pragma unroll
-    for(int k = 0; k < N; k++)
-        y[k] = 0;
-#pragma unroll
-    for(int i = 0; i < N; i++)
-    {
-        const uint32_t xi = x[i];
-#pragma unroll 8
-        for(int b = 0; b < 32; b++)
-        {
-            const uint32_t  mask = 0u - ((xi >> b) & 1u);
-            const uint32_t* row  = m + (i * 32 + b) * N;
-#pragma unroll
-            for(int k = 0; k < N; k++)
-                y[k] ^= mask & __ldg(row + k);
-        }
-    }
-#pragma unroll
-    for(int k = 0; k < N; k++)
-        x[k] = y[k];
-}
-
-__device__ __forceinline__ void mod_apply(const uint64_t* __restrict__ a, uint64_t m, uint32_t* x)
-{
-    uint32_t y[3];
-#pragma unroll
-    for(int r = 0; r < 3; r++)
-    {
-        uint64_t s = 0;
-#pragma unroll
-        for(int c = 0; c < 3; c++)
-            s += (__ldg(reinterpret_cast<const unsigned long long*>(a) + r * 3 + c) * x[c]) % m;
-        y[r] = static_cast<uint32_t>(s % m);
-    }
-#pragma unroll
-    for(int r = 0; r < 3; r++)
-        x[r] = y[r];
-}
 
 struct InitArgs
 {
@@ -251,31 +106,6 @@ struct FillArgs
     unsigned long long n, vec_n;
 };
 
-template<class T, unsigned N>
-__device__ __forceinline__ void store_small(unsigned char* p, const T (&v)[N])
-{
-    constexpr unsigned VB = sizeof(T) * N;
-    if constexpr(VB == 4)
-    {
-        uint32_t w;
-        memcpy(&w, v, 4);
-        __stcs(reinterpret_cast<unsigned int*>(p), w);
-    }
-    else if constexpr(VB == 8)
-    {
-        uint2 w;
-        memcpy(&w, v, 8);
-        __stcs(reinterpret_cast<uint2*>(p), w);
-    }
-    else
-    {
-        static_assert(VB == 16, "vector size");
-        uint4 w;
-        memcpy(&w, v, 16);
-        __stcs(reinterpret_cast<uint4*>(p), w);
-    }
-}
-
 template<class E, class F>
 __global__ void __launch_bounds__(kBlock) stateful_fill(FillArgs a, F f)
 {
@@ -336,13 +166,7 @@ __global__ void __launch_bounds__(kBlock) stateful_fill(FillArgs a, F f)
 // ---------------------------------------------------------------------------------------
 // Host side: seeding, base states and tables.
 
-enum class Family
-{
-    XORWOW,
-    MRG32K3A,
-    MRG31K3P,
-    LFSR113
-};
+using Family = StatefulFamily;
 
 // Device copies of the per-digit jump tables, one upload per (family, device).
 struct DeviceTables
@@ -538,6 +362,43 @@ static void seeded_state(Family fam, unsigned long long seed, uint4 seed4, uint3
     }
 }
 
+// Base states of engine 0 for engines >= offset % E (base[0]: offset / E steps) and below
+// it (base[1]: one step more), xorwow.hpp:45-61 and siblings.
+static void bases_of(Family fam, unsigned long long seed, uint4 seed4, unsigned long long offset,
+                     uint32_t (&base)[2][6])
+{
+    unsigned long long jump = offset / kE;
+    if(fam == Family::LFSR113)
+        jump = static_cast<uint32_t>(jump); // init_lfsr113_engines takes a 32-bit offset
+    seeded_state(fam, seed, seed4, base[0]);
+    host_discard(fam, base[0], jump);
+    std::memcpy(base[1], base[0], sizeof(base[0]));
+    if(fam == Family::LFSR113)
+    {
+        // engines below start skip (uint32)(offset/E) + 1, computed in 32 bits
+        seeded_state(fam, seed, seed4, base[1]);
+        host_discard(fam, base[1], static_cast<uint32_t>(static_cast<uint32_t>(jump) + 1u));
+    }
+    else
+    {
+        host_discard(fam, base[1], 1);
+    }
+}
+
+StatefulBases stateful_bases(StatefulFamily fam, unsigned long long seed, unsigned long long offset)
+{
+    StatefulBases b{};
+    uint4         seed4 = make_uint4(2u, 8u, 16u, 128u); // lfsr113.hpp:178-186
+    bases_of(fam, seed, seed4, offset, b.base);
+    b.start = static_cast<uint32_t>(offset % kE);
+    return b;
+}
+
+const void* stateful_digit_tables(StatefulFamily fam)
+{
+    return digit_tables(fam);
+}
+
 template<Family kFam>
 class StatefulGenerator final : public PseudoGeneratorBase
 {
@@ -641,25 +502,10 @@ public:
             }
         }
         m_start = static_cast<uint32_t>(m_offset % kE);
-        unsigned long long jump = m_offset / kE;
-        if constexpr(kFam == Family::LFSR113)
-            jump = static_cast<uint32_t>(jump); // init_lfsr113_engines takes a 32-bit offset
         InitArgs a{};
         a.start = m_start;
         a.arena = m_arena;
-        seeded_state(kFam, m_seed, m_seed4, a.base[0]);
-        host_discard(kFam, a.base[0], jump);
-        std::memcpy(a.base[1], a.base[0], sizeof(a.base[0]));
-        if constexpr(kFam == Family::LFSR113)
-        {
-            // engines below start skip (uint32)(offset/E) + 1, computed in 32 bits
-            seeded_state(kFam, m_seed, m_seed4, a.base[1]);
-            host_discard(kFam, a.base[1], static_cast<uint32_t>(static_cast<uint32_t>(jump) + 1u));
-        }
-        else
-        {
-            host_discard(kFam, a.base[1], 1);
-        }
+        bases_of(kFam, m_seed, m_seed4, m_offset, a.base);
         const void* tables = digit_tables(kFam);
         if(tables == nullptr)
             return ROCRAND_STATUS_ALLOCATION_FAILED;

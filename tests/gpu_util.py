@@ -78,8 +78,42 @@ def ulp_diff(a, b):
     return np.abs(_mono(a) - _mono(b))
 
 
-def compare(dist, got, exp, params=()):
-    """Asserts parity of one output; returns the max ulp distance (0 for bit-exact)."""
+def _ratios(dist, got, exp, params):
+    """Per-element error / allowed error of one output against one expectation (0 where
+    both are the same non-finite value, inf where only one is finite)."""
+    tol = ULP_TOL[dist]
+    mean = float(params[0]) if params else 0.0
+    T = exp.dtype.type
+    ratio = np.full(exp.shape, np.inf)
+    same = (got.view(np.uint8).reshape(exp.size, -1) == exp.view(np.uint8).reshape(exp.size, -1)).all(axis=1)
+    ratio[same] = 0.0
+    fin = np.isfinite(exp) & np.isfinite(got) & ~same
+    g, e = got[fin], exp[fin]
+
+    def sp(x):  # ulp of |x| in the output precision, as float64
+        return np.spacing(np.abs(x).astype(exp.dtype)).astype(np.float64)
+
+    if not e.size:
+        return ratio
+    if dist.startswith("log_normal"):
+        pos = (e > 0) & (g > 0)
+        r = np.full(e.shape, np.inf)
+        z = np.log(e[pos].astype(np.float64))
+        err = np.abs(np.log(g[pos].astype(np.float64)) - z)
+        lim = tol * sp(z - mean) + sp(z) + 2 * float(np.spacing(T(1)))
+        r[pos] = err / lim
+    else:
+        err = np.abs(g.astype(np.float64) - e.astype(np.float64))
+        lim = tol * sp(e.astype(np.float64) - mean) + (sp(e) if mean != 0.0 else 0.0)
+        lim = np.maximum(lim, np.finfo(exp.dtype).smallest_subnormal)
+        r = err / lim
+    ratio[fin] = r
+    return ratio
+
+
+def compare(dist, got, exp, params=(), alts=()):
+    """Asserts parity of one output; returns the max ulp distance (0 for bit-exact).
+    Elements outside the tolerance of `exp` may instead be within it of one of `alts`."""
     assert got.shape == exp.shape
     if dist in BIT_EXACT:
         if not np.array_equal(got.view(np.uint8), exp.view(np.uint8)):
@@ -87,35 +121,51 @@ def compare(dist, got, exp, params=()):
             raise AssertionError("%s: %d mismatches, first at %s: got %r want %r" % (
                 dist, bad.size, bad[:5], got[bad[:5]], exp[bad[:5]]))
         return 0
-    same_nonfinite = np.isfinite(got) == np.isfinite(exp)
-    assert same_nonfinite.all(), "%s: finite/non-finite mismatch" % dist
-    fin = np.isfinite(exp) & np.isfinite(got)
-    g, e = got[fin], exp[fin]
-    if not e.size:
+    if not exp.size:
         return 0
-    tol = ULP_TOL[dist]
-    mean = float(params[0]) if params else 0.0
-    T = e.dtype.type
-
-    def sp(x):  # ulp of |x| in the output precision, as float64
-        return np.spacing(np.abs(x).astype(e.dtype)).astype(np.float64)
-
-    if dist.startswith("log_normal"):
-        pos = (e > 0) & (g > 0)
-        assert pos.all() or np.array_equal(g[~pos], e[~pos]), "%s: sign/zero mismatch" % dist
-        z = np.log(e[pos].astype(np.float64))
-        err = np.abs(np.log(g[pos].astype(np.float64)) - z)
-        lim = tol * sp(z - mean) + sp(z) + 2 * float(np.spacing(T(1)))
-        ratio = err / lim
-        worst_ulps = int(ulp_diff(g, e).max())
-    else:
-        err = np.abs(g.astype(np.float64) - e.astype(np.float64))
-        lim = tol * sp(e.astype(np.float64) - mean) + (sp(e) if mean != 0.0 else 0.0)
-        lim = np.maximum(lim, np.finfo(e.dtype).smallest_subnormal)
-        ratio = err / lim
-        worst_ulps = int(ulp_diff(g, e).max())
-    if ratio.size and (ratio > 1.0).any():
+    ratio = _ratios(dist, got, exp, params)
+    for alt in alts:
+        ratio = np.minimum(ratio, _ratios(dist, got, alt, params))
+    fin = np.isfinite(exp) & np.isfinite(got)
+    worst_ulps = int(ulp_diff(got[fin], exp[fin]).max()) if fin.any() else 0
+    if (ratio > 1.0).any():
         k = int(np.argmax(ratio))
-        raise AssertionError("%s: error %.3g > limit %.3g at %d (got %r want %r); max output ulp %d" % (
-            dist, err[k], lim[k], k, g[k], e[k], worst_ulps))
+        raise AssertionError("%s: %d outside tolerance, worst %.3g x limit at %d (got %r want %r); "
+                             "max output ulp %d" % (dist, int((ratio > 1.0).sum()), ratio[k], k,
+                                                    got[k], exp[k], worst_ulps))
     return worst_ulps
+
+
+SOBOL = {501, 502, 504, 505}
+
+
+def erfinv_normal(rng, dist):
+    """Whether the reference computes this normal / log-normal by its inverse-erf formula
+    (Sobol: normal.hpp:272-330; ThreeFry2x32 fp64: threefry.hpp:441-449)."""
+    if dist not in ULP_TOL:
+        return False
+    return rng in SOBOL or (rng == 408 and dist in ("normal_double", "log_normal_double"))
+
+
+def compare_call(orc, rng, seed, offset, dims, calls, k, got, exp):
+    """compare() for call k of a sequence.  The inverse-erf normal computes
+    sqrt(-tt1 + sqrt(tt1^2 - tt2)) with tt1, tt2 linear in log(x): the subtraction cancels,
+    so an output moves by tens of ulps when log(x) moves by one.  Where the reference uses
+    it, an element outside the ulp tolerance must instead be within it of the reference
+    formula evaluated at the host's logarithm moved by one ulp either way (the oracle rerun
+    with that logarithm): the device's logarithm is correctly rounded, the host library's
+    is within one ulp."""
+    dist, _, params, _ = calls[k]
+    try:
+        return compare(dist, got, exp, params)
+    except AssertionError:
+        if not erfinv_normal(rng, dist):
+            raise
+    alts = []
+    for shift in (1, -1):
+        orc.set_erfinv_log_ulps(shift)
+        try:
+            alts.append(pyorc.run_sequence(orc, rng, seed, offset, calls[:k + 1], dims=dims)[k][1])
+        finally:
+            orc.set_erfinv_log_ulps(0)
+    return compare(dist, got, exp, params, alts)

@@ -96,3 +96,23 @@ def test_discrete_null_arguments(lib):
     assert lib.rocrand_create_poisson_distribution(0.0, ctypes.byref(out)) == rb.ROCRAND_STATUS_OUT_OF_RANGE
     assert lib.rocrand_create_discrete_distribution(None, 0, 0, ctypes.byref(out)) == rb.ROCRAND_STATUS_OUT_OF_RANGE
     assert lib.rocrand_destroy_discrete_distribution(None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+
+
+def test_mt19937_host_side_semantics(lib):
+    """MT19937 (mt19937.hpp:758-780, 1044-1060): no offset, orderings DEFAULT/BEST/LEGACY
+    only, no 64-bit output; all refused before any device work."""
+    st, g = _create(lib, rb.ROCRAND_RNG_PSEUDO_MT19937)
+    assert st == 0
+    try:
+        assert lib.rocrand_set_offset(g, 5) == rb.ROCRAND_STATUS_TYPE_ERROR
+        assert lib.rocrand_set_offset(g, 0) == rb.ROCRAND_STATUS_TYPE_ERROR
+        for o in (rb.ROCRAND_ORDERING_PSEUDO_DYNAMIC, rb.ROCRAND_ORDERING_PSEUDO_SEEDED,
+                  rb.ROCRAND_ORDERING_QUASI_DEFAULT):
+            assert lib.rocrand_set_ordering(g, o) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+        for o in (100, 101, 103):
+            assert lib.rocrand_set_ordering(g, o) == 0
+        assert lib.rocrand_generate_long_long(g, None, 10) == rb.ROCRAND_STATUS_TYPE_ERROR
+        assert lib.rocrand_set_seed(g, 0) == 0
+        assert lib.rocrand_set_quasi_random_generator_dimensions(g, 2) == rb.ROCRAND_STATUS_TYPE_ERROR
+    finally:
+        assert lib.rocrand_destroy_generator(g) == 0

@@ -22,7 +22,8 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 PSEUDO = {"philox": 404, "threefry2x32": 408, "threefry2x64": 409, "threefry4x32": 410,
-          "threefry4x64": 411, "xorwow": 401, "mrg32k3a": 402, "mrg31k3p": 405, "lfsr113": 406}
+          "threefry4x64": 411, "xorwow": 401, "mrg32k3a": 402, "mrg31k3p": 405, "lfsr113": 406,
+          "mt19937": 407}
 WORD64 = {"threefry2x64", "threefry4x64"}
 STATEFUL = {"xorwow", "mrg32k3a", "mrg31k3p", "lfsr113"}
 
@@ -41,15 +42,17 @@ def test_golden_replay(lib, orc, name):
         g = gu.create(lib, case["rng"], case.get("seed"), case.get("offset"), case.get("dims"))
         ref = pyorc.run_sequence(orc, case["rng"], case.get("seed"), case.get("offset"),
                                  [tuple(c) for c in case["calls"]], dims=case.get("dims"))
+        calls = [tuple(c) for c in case["calls"]]
         try:
-            for (dist, n, params, mis), exp, (ost, ovals) in zip(case["calls"], case["results"], ref):
+            for k, ((dist, n, params, mis), exp, (ost, ovals)) in enumerate(zip(calls, case["results"], ref)):
                 st, vals = gu.device_generate(lib, g, dist, n, params, mis)
                 assert st == exp["status"] == ost
                 if st != 0:
                     continue
                 if dist in gu.BIT_EXACT:
                     assert gu.sha(vals) == exp["sha256"], (name, dist, n, mis)
-                gu.compare(dist, vals, ovals, params)
+                gu.compare_call(orc, case["rng"], case.get("seed"), case.get("offset"), case.get("dims"),
+                                calls, k, vals, ovals)
         finally:
             lib.rocrand_destroy_generator(g)
 
@@ -69,6 +72,8 @@ def test_random_sequences(lib, orc, name, dist, params):
     rng = np.random.default_rng(zlib.crc32(repr((name, dist, params)).encode()))
     seed = int(rng.integers(0, 2**63))
     offset = int(rng.integers(0, 2**20)) if rng.random() < 0.5 else 0
+    if name == "mt19937":
+        offset = None  # MT19937 has no offset (set_offset is a TYPE_ERROR)
     calls = []
     for n in (1 << 20, 3, int(rng.integers(1, 100000)), (1 << 18) + 5):
         calls.append((dist, n, params, int(rng.integers(0, 16))))
@@ -77,14 +82,47 @@ def test_random_sequences(lib, orc, name, dist, params):
     worst = 0
     expect_status = 103 if (dist == "ulonglong" and name not in WORD64) else 0
     try:
-        for (d, n, p, mis), (ost, ovals) in zip(calls, ref):
+        for k, ((d, n, p, mis), (ost, ovals)) in enumerate(zip(calls, ref)):
             st, vals = gu.device_generate(lib, g, d, n, p, mis)
             assert st == ost == expect_status
             if st == 0:
-                worst = max(worst, gu.compare(d, vals, ovals, p))
+                worst = max(worst, gu.compare_call(orc, PSEUDO[name], seed, offset, None, calls, k,
+                                                   vals, ovals))
     finally:
         lib.rocrand_destroy_generator(g)
     print("%s %s max ulp %d" % (name, dist, worst))
+
+
+MT_MIX = ["uint", "char", "short", "uniform", "uniform_double", "uniform_half", "normal",
+          "normal_double", "normal_half", "log_normal", "log_normal_double", "log_normal_half",
+          "poisson"]
+
+
+@pytest.mark.parametrize("seed", [7, 0xfeedface12345])
+def test_mt19937_mixed_sequences(lib, orc, seed):
+    """MT19937 keeps one state across calls of different input widths: a random sequence of
+    distributions, sizes and alignments (calls served from the previous call's state, calls
+    crossing twists, width changes that skip slot groups) must equal the oracle."""
+    rng = np.random.default_rng(seed)
+    calls = []
+    for _ in range(40):
+        d = MT_MIX[int(rng.integers(0, len(MT_MIX)))]
+        p = {"normal": [0.5, 2.0], "normal_double": [-1.0, 0.5], "normal_half": [1.0, 2.0],
+             "log_normal": [0.2, 0.7], "log_normal_double": [0.1, 0.4],
+             "log_normal_half": [0.0, 0.5],
+             "poisson": [float(rng.choice([0.5, 10.0, 5000.5]))]}.get(d, [])
+        n = int(rng.choice([int(rng.integers(0, 70)), int(rng.integers(0, 300000)),
+                            int(rng.integers(0, 3000000))]))
+        calls.append((d, n, p, int(rng.integers(0, 16))))
+    g = gu.create(lib, PSEUDO["mt19937"], seed)
+    ref = pyorc.run_sequence(orc, PSEUDO["mt19937"], seed, None, calls)
+    try:
+        for (d, n, p, mis), (ost, ovals) in zip(calls, ref):
+            st, vals = gu.device_generate(lib, g, d, n, p, mis)
+            assert st == ost == 0
+            gu.compare(d, vals, ovals, p)
+    finally:
+        lib.rocrand_destroy_generator(g)
 
 
 @pytest.mark.parametrize("name", sorted(PSEUDO))
@@ -95,16 +133,17 @@ def test_full_size_against_oracle_and_continuity(lib, orc, name, dist):
     import torch
     n = 1 << 28
     params = [0.0, 1.0] if dist == "normal" else []
-    g = gu.create(lib, PSEUDO[name], 0xdeadbeef, 0)
+    offset = None if name == "mt19937" else 0
+    g = gu.create(lib, PSEUDO[name], 0xdeadbeef, offset)
     st, big = gu.device_generate(lib, g, dist, n, params, 0)
     assert st == 0
     lib.rocrand_destroy_generator(g)
-    ost, ovals = pyorc.run_sequence(orc, PSEUDO[name], 0xdeadbeef, 0, [(dist, n, params, 0)])[0]
+    ost, ovals = pyorc.run_sequence(orc, PSEUDO[name], 0xdeadbeef, offset, [(dist, n, params, 0)])[0]
     assert ost == 0
-    gu.compare(dist, big, ovals, params)
+    gu.compare_call(orc, PSEUDO[name], 0xdeadbeef, offset, None, [(dist, n, params, 0)], 0, big, ovals)
     del ovals
     # continuity: 3 calls of the same total
-    g = gu.create(lib, PSEUDO[name], 0xdeadbeef, 0)
+    g = gu.create(lib, PSEUDO[name], 0xdeadbeef, offset)
     parts = [(1 << 27) + 12, (1 << 26) - 4, n - (1 << 27) - (1 << 26) - 8]
     got = []
     for k in parts:
@@ -133,11 +172,12 @@ def test_quasi_random_sequences(lib, orc, name, dist, params):
     expect_status = 103 if (dist == "ulonglong" and is32) else 0
     worst = 0
     try:
-        for (d, n, p, mis), (ost, ovals) in zip(calls, ref):
+        for k, ((d, n, p, mis), (ost, ovals)) in enumerate(zip(calls, ref)):
             st, vals = gu.device_generate(lib, g, d, n, p, mis)
             assert st == ost == expect_status
             if st == 0:
-                worst = max(worst, gu.compare(d, vals, ovals, p))
+                worst = max(worst, gu.compare_call(orc, QUASI[name], None, offset, dims, calls, k,
+                                                   vals, ovals))
     finally:
         lib.rocrand_destroy_generator(g)
     print("%s %s dims=%d max ulp %d" % (name, dist, dims, worst))
@@ -159,6 +199,6 @@ def test_quasi_config_sizes(lib, orc, name, dims, dist):
     assert st == 0
     ost, ovals = pyorc.run_sequence(orc, QUASI[name], None, 4096, [(dist, n, params, 0)], dims=dims)[0]
     assert ost == 0
-    gu.compare(dist, vals, ovals, params)
+    gu.compare_call(orc, QUASI[name], None, 4096, dims, [(dist, n, params, 0)], 0, vals, ovals)
     del vals, ovals
     torch.cuda.empty_cache()
