@@ -54,8 +54,9 @@ float    orc_half_to_float(uint16_t h);
  * discrete.hpp normalize + create_alias_table).  Returns size; prob/alias need >= capacity. */
 unsigned orc_poisson_table(double lambda, double* prob, uint32_t* alias, unsigned* offset);
 unsigned orc_poisson_capacity(double lambda);
-/* Moves the logarithm of the inverse-erf normal by k ulps (see orc_internal.h). */
-void orc_set_erfinv_log_ulps(int k);
+/* Moves the host library's log and sin/cos results of the fp64 normal transforms by the
+ * given numbers of ulps (test hook, see orc_internal.h; 0, 0 restores). */
+void orc_set_libm_ulps(int log_ulps, int trig_ulps);
 
 #ifdef __cplusplus
 }

@@ -101,9 +101,9 @@ static void box_muller_d(uint32_t x, uint32_t y, uint32_t z, uint32_t w, double 
     const double   u  = ORC_2POW53_INV_DOUBLE + (v1 * ORC_2POW53_INV_DOUBLE);
     const uint64_t v2 = (uint64_t)z ^ ((uint64_t)w << (53 - 32));
     const double   ww = (ORC_2POW53_INV_DOUBLE * 2.0) + (v2 * (ORC_2POW53_INV_DOUBLE * 2.0));
-    const double   s  = sqrt(-2.0 * log(u));
-    r[0]              = sin(ww * ORC_PI_DOUBLE) * s;
-    r[1]              = cos(ww * ORC_PI_DOUBLE) * s;
+    const double   s  = sqrt(-2.0 * orc_log_shift_d(log(u)));
+    r[0]              = orc_shift_d(sin(ww * ORC_PI_DOUBLE), orc_trig_ulps) * s;
+    r[1]              = orc_shift_d(cos(ww * ORC_PI_DOUBLE), orc_trig_ulps) * s;
 }
 
 /* rocrand_normal.h:102-122, branch without half math (the host build) */
@@ -116,9 +116,14 @@ static void box_muller_h(uint16_t x, uint16_t y, uint16_t r[2])
     r[1]          = orc_float_to_half(cosf(v) * s);
 }
 
-int orc_erfinv_log_ulps = 0;
+int orc_log_ulps  = 0;
+int orc_trig_ulps = 0;
 
-void orc_set_erfinv_log_ulps(int k) { orc_erfinv_log_ulps = k; }
+void orc_set_libm_ulps(int log_ulps, int trig_ulps)
+{
+    orc_log_ulps  = log_ulps;
+    orc_trig_ulps = trig_ulps;
+}
 
 /* rocrand_normal.h:196-220 roc_d_erfinv */
 static double erfinv_d(double x)
@@ -187,9 +192,9 @@ static void mrg_box_muller_d(int mrg, uint32_t x, uint32_t y, double r[2])
 {
     const double u = mrg_f(mrg, x);
     const double v = mrg_f(mrg, y) * 2.0;
-    const double s = sqrt(-2.0 * log(u));
-    r[0]           = sin(v * ORC_PI_DOUBLE) * s;
-    r[1]           = cos(v * ORC_PI_DOUBLE) * s;
+    const double s = sqrt(-2.0 * orc_log_shift_d(log(u)));
+    r[0]           = orc_shift_d(sin(v * ORC_PI_DOUBLE), orc_trig_ulps) * s;
+    r[1]           = orc_shift_d(cos(v * ORC_PI_DOUBLE), orc_trig_ulps) * s;
 }
 
 static void mrg_apply(const orc_dist* d, const uint32_t* in, void* outv)

@@ -197,24 +197,30 @@ struct orc_gen {
 
 static inline size_t orc_min_sz(size_t a, size_t b) { return a < b ? a : b; }
 
-/* Test hook: the logarithm inside the inverse-erf normal (rocrand_normal.h:174-226) moved
- * by this many ulps (0 = the reference's value).  The formula -tt1 + sqrt(tt1^2 - tt2)
- * cancels, so one ulp of log moves the normal by many ulps; a test accepts a device value
- * that equals the formula at a neighbouring logarithm. */
-extern int orc_erfinv_log_ulps;
+/* Test hook: the host library's logarithm (inside the inverse-erf normal,
+ * rocrand_normal.h:174-226, and the fp64 Box-Muller transforms, :68-89, 154-172) and its
+ * sine/cosine (fp64 Box-Muller) moved by this many ulps (0 = the reference's values).  A
+ * test accepts a device value that equals the reference formula at neighbouring values of
+ * these transcendentals: the inverse-erf formula -tt1 + sqrt(tt1^2 - tt2) cancels, and the
+ * Box-Muller products can turn one ulp of sin into two of the output. */
+extern int orc_log_ulps;
+extern int orc_trig_ulps;
 
-static inline float orc_log_shift_f(float v)
+static inline float orc_shift_f(float v, int k)
 {
-    for(int k = orc_erfinv_log_ulps; k != 0 && isfinite(v) && v != 0.0f; k += k > 0 ? -1 : 1)
+    for(; k != 0 && isfinite(v) && v != 0.0f; k += k > 0 ? -1 : 1)
         v = nextafterf(v, k > 0 ? INFINITY : -INFINITY);
     return v;
 }
 
-static inline double orc_log_shift_d(double v)
+static inline double orc_shift_d(double v, int k)
 {
-    for(int k = orc_erfinv_log_ulps; k != 0 && isfinite(v) && v != 0.0; k += k > 0 ? -1 : 1)
+    for(; k != 0 && isfinite(v) && v != 0.0; k += k > 0 ? -1 : 1)
         v = nextafter(v, k > 0 ? INFINITY : -INFINITY);
     return v;
 }
+
+static inline float orc_log_shift_f(float v) { return orc_shift_f(v, orc_log_ulps); }
+static inline double orc_log_shift_d(double v) { return orc_shift_d(v, orc_log_ulps); }
 
 #endif

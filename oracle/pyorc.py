@@ -80,9 +80,10 @@ class CLib:
             f = getattr(self.lib, self.prefix + fn)
             f.argtypes = [c_void_p, c_ulonglong]
 
-    def set_erfinv_log_ulps(self, k):
-        """Oracle only: moves the inverse-erf normal's logarithm by k ulps (0 restores)."""
-        self.lib.orc_set_erfinv_log_ulps(ctypes.c_int(k))
+    def set_libm_ulps(self, log_ulps, trig_ulps=0):
+        """Oracle only: moves the host library's log and sin/cos results of the fp64 normal
+        transforms (and the inverse-erf normal's log) by these many ulps (0, 0 restores)."""
+        self.lib.orc_set_libm_ulps(ctypes.c_int(log_ulps), ctypes.c_int(trig_ulps))
 
     def fn(self, name):
         return getattr(self.lib, self.prefix + name)
