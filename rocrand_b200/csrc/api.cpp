@@ -36,7 +36,9 @@ const DeviceInfo& device_info()
     return cache[dev];
 }
 
-static rocrand_generator_base_type* make_generator(rocrand_rng_type t)
+namespace rb200
+{
+rocrand_generator_base_type* make_generator(rocrand_rng_type t)
 {
     switch(t)
     {
@@ -59,6 +61,7 @@ static rocrand_generator_base_type* make_generator(rocrand_rng_type t)
         default: return nullptr;
     }
 }
+} // namespace rb200
 
 template<class Fn>
 static rocrand_status guarded(Fn&& fn)

@@ -1,0 +1,124 @@
+// batch.hpp -- many generators in one launch: host side of the work-descriptor table.
+//
+// A batch is a list of requests; each request is what one rocrand_generate_* call writes
+// (a fresh generator of that type, seed and offset, or a resident generator state).  The
+// host turns each request into a descriptor (engine position, distribution parameters,
+// output layout exactly as the plain call would lay it out) and cuts it into tiles; one
+// persistent kernel then lets every block take the next tile from a global counter.
+#pragma once
+
+#include "common.hpp"
+#include "counter_engines.cuh"
+#include "generators.hpp"
+
+#include <vector>
+
+namespace rb200
+{
+
+enum BatchKind : uint32_t
+{
+    BK_PHILOX   = 0,
+    BK_XORWOW   = 1,
+    BK_MRG32K3A = 2,
+    BK_SOBOL32  = 3,
+    BK_COUNT    = 4
+};
+
+enum BatchDist : uint32_t
+{
+    BD_UINT     = 0,
+    BD_FLOAT    = 1,
+    BD_DOUBLE   = 2,
+    BD_NORMAL_F = 3,
+    BD_POISSON  = 4,
+    BD_COUNT    = 5
+};
+
+// Position of the Philox output contract of one plain call (see philox.cu).
+struct BatchPhilox
+{
+    PhiloxKeys keys;
+    uint4      c0;
+    uint32_t   s0, head, start0, tail;
+};
+
+// One request as the kernel sees it.
+struct BatchReq
+{
+    uint32_t           kind, dist;
+    unsigned char*     data;  // output base
+    unsigned char*     vec;   // first aligned vector (Philox / stateful)
+    unsigned long long n;     // elements
+    unsigned long long vec_n; // Philox: 16-byte vectors; stateful: ow-vectors; Sobol: points
+    unsigned long long tile0; // first global tile
+    uint32_t           units; // vectors / slots / points per tile
+    uint32_t           head, tail;
+    // distribution
+    float         mean, stddev;
+    const double* prob;
+    const uint32_t* alias;
+    const double* cdf;
+    uint32_t      tsize, toff, huge;
+    double        lambda, sqrt_lambda;
+    // engines
+    BatchPhilox     philox;
+    uint32_t        base[2][6]; // stateful: engines >= start / below start
+    uint32_t        start;
+    uint32_t*       arena;      // stateful resident state (nullptr: fresh, seeded from base)
+    uint32_t        sobol_offset;
+    const uint32_t* sobol_v;    // the 32 direction vectors of dimension 0
+};
+
+// Tile sizes and grid of one (kind, dist) pair, chosen by the autotuner.
+struct BatchTuning
+{
+    uint32_t units[BK_COUNT][BD_COUNT];
+    uint32_t blocks_per_sm;
+};
+
+// Default tile sizes, replaced by rocrand_b200_autotune_batch on a device.
+BatchTuning& batch_tuning();
+
+// A request of the public ABI turned into descriptors; owns the device table.
+class BatchPlan
+{
+public:
+    ~BatchPlan();
+    // Validates and lays out the requests (fresh generators); Poisson tables are made
+    // resident on `stream`.
+    rocrand_status build(const void* requests, size_t count, cudaStream_t stream);
+    // Appends one already-built descriptor (resident generators, used by the server).
+    void add(const BatchReq& r) { m_reqs.push_back(r); }
+    // Drops the descriptors, keeping the device table for reuse.
+    void clear() { m_reqs.clear(); }
+    // Assigns tiles and uploads the table on `stream`.
+    rocrand_status upload(cudaStream_t stream);
+    // Launches the persistent kernel (resets the tile counter first).
+    rocrand_status launch(cudaStream_t stream);
+    // Replays a captured graph of reset + launch (captured on first use).
+    rocrand_status replay(cudaStream_t stream);
+    size_t requests() const { return m_reqs.size(); }
+    unsigned long long bytes() const { return m_bytes; }
+
+private:
+    std::vector<BatchReq> m_reqs;
+    unsigned long long    m_tiles   = 0;
+    unsigned long long    m_bytes   = 0;
+    BatchReq*             d_reqs    = nullptr;
+    unsigned long long*   d_next    = nullptr;
+    size_t                m_cap     = 0;
+    cudaGraphExec_t       m_exec    = nullptr;
+    int                   m_device  = -1;
+};
+
+// Fills the distribution fields of a descriptor (Poisson tables are cached per lambda).
+rocrand_status batch_set_dist(BatchReq& r, uint32_t dist, double p0, double p1, cudaStream_t stream);
+// Output layout of one plain call (head, vectors, tail) for the request's kind and dist.
+rocrand_status batch_layout(BatchReq& r, void* output, size_t n);
+// Bytes per output element.
+uint32_t batch_elem_size(uint32_t dist);
+// Engine values consumed (iw) and outputs written (ow) per distribution call.
+void batch_widths(uint32_t kind, uint32_t dist, unsigned& iw, unsigned& ow);
+
+} // namespace rb200

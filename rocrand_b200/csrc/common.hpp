@@ -84,6 +84,8 @@ struct DeviceInfo
 };
 const DeviceInfo& device_info();
 
+struct BatchReq; // batch.hpp
+
 } // namespace rb200
 
 // Base of every generator: the opaque handle type of the C ABI.
@@ -116,6 +118,16 @@ struct rocrand_generator_base_type
     virtual rocrand_status generate(void* data, size_t n, rb200::Dist d, const rb200::DistParams& p)
         = 0;
     virtual rocrand_status generate_poisson(unsigned int* data, size_t n, double lambda) = 0;
+    // Batched-fill form of the next call: describes `n` values of batch distribution `dist`
+    // (batch.hpp) into `data` as a descriptor of the batch kernel, from the generator's
+    // current state, and advances the state exactly as that call would.  Poisson tables are
+    // made resident on `stream`.  TYPE_ERROR where the generator has no batched form.
+    virtual rocrand_status batch_descriptor(uint32_t dist, double p0, double p1, void* data,
+                                            size_t n, rb200::BatchReq& r, cudaStream_t stream)
+    {
+        (void)dist, (void)p0, (void)p1, (void)data, (void)n, (void)r, (void)stream;
+        return ROCRAND_STATUS_TYPE_ERROR;
+    }
 
     cudaStream_t stream() const { return m_stream; }
 

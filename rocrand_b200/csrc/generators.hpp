@@ -44,6 +44,8 @@ public:
     rocrand_status   set_order(rocrand_ordering order) override;
     rocrand_status   generate(void* data, size_t n, Dist d, const DistParams& p) override;
     rocrand_status   generate_poisson(unsigned int* data, size_t n, double lambda) override;
+    rocrand_status   batch_descriptor(uint32_t dist, double p0, double p1, void* data, size_t n,
+                                      BatchReq& r, cudaStream_t stream) override;
 
 private:
     CounterPos m_pos;
@@ -74,6 +76,9 @@ struct StatefulBases
 StatefulBases stateful_bases(StatefulFamily fam, unsigned long long seed, unsigned long long offset);
 // Per-digit subsequence jump tables of a family on the current device (uploaded once).
 const void* stateful_digit_tables(StatefulFamily fam);
+
+// Generator of any type (api.cpp); nullptr for an unknown type.
+rocrand_generator_base_type* make_generator(rocrand_rng_type t);
 
 // Factories of the other generator families (one translation unit each).
 rocrand_generator_base_type* make_threefry(rocrand_rng_type t);

@@ -19,6 +19,7 @@
 #include "dist.cuh"
 #include "generators.hpp"
 #include "launch.cuh"
+#include "batch.hpp"
 #include "philox.cuh"
 #include "poisson.hpp"
 
@@ -239,6 +240,28 @@ rocrand_status philox_poisson_with_table(unsigned long long seed, unsigned long 
     if(p.huge)
         return launch_philox(a, FnPoissonHuge{p.sqrt_lambda, p.lambda}, stream);
     return launch_philox(a, FnPoisson{p.prob, p.alias, p.size, p.offset}, stream);
+}
+
+rocrand_status PhiloxGenerator::batch_descriptor(uint32_t dist, double p0, double p1, void* data,
+                                                size_t n, BatchReq& r, cudaStream_t stream)
+{
+    rocrand_status st = init();
+    if(st != ROCRAND_STATUS_SUCCESS)
+        return st;
+    r             = BatchReq{};
+    r.kind        = BK_PHILOX;
+    r.philox.keys = philox_keys(m_seed);
+    r.philox.c0   = m_pos.counter;
+    r.philox.s0   = m_pos.sub;
+    st            = batch_set_dist(r, dist, p0, p1, stream);
+    if(st == ROCRAND_STATUS_SUCCESS)
+        st = batch_layout(r, data, n);
+    if(st != ROCRAND_STATUS_SUCCESS)
+        return st;
+    unsigned iw, ow;
+    batch_widths(BK_PHILOX, dist, iw, ow);
+    m_pos.advance(static_cast<unsigned long long>((n + ow - 1) / ow) * iw);
+    return ROCRAND_STATUS_SUCCESS;
 }
 
 rocrand_status PhiloxGenerator::generate_poisson(unsigned int* data, size_t n, double lambda)

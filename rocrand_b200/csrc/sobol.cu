@@ -18,6 +18,7 @@
 #include "generators.hpp"
 #include "launch.cuh"
 #include "poisson.hpp"
+#include "batch.hpp"
 #include "sobol_dist.cuh"
 #include "sobol_tables.hpp"
 
@@ -168,6 +169,29 @@ public:
             return ROCRAND_STATUS_OUT_OF_RANGE;
         m_dims        = dims;
         m_initialized = false;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    rocrand_status batch_descriptor(uint32_t dist, double p0, double p1, void* data, size_t n,
+                                    BatchReq& r, cudaStream_t stream) override
+    {
+        if(kIs64 || kScrambled || m_dims != 1)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        rocrand_status st = init();
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        r              = BatchReq{};
+        r.kind         = BK_SOBOL32;
+        r.sobol_offset = m_current;
+        r.sobol_v      = static_cast<const uint32_t*>(sobol_device_vectors(false, false));
+        if(r.sobol_v == nullptr)
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        st = batch_set_dist(r, dist, p0, p1, stream);
+        if(st == ROCRAND_STATUS_SUCCESS)
+            st = batch_layout(r, data, n);
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        m_current += static_cast<uint32_t>(n);
         return ROCRAND_STATUS_SUCCESS;
     }
 

@@ -25,6 +25,7 @@
 #include "launch.cuh"
 #include "poisson.hpp"
 #include "stateful_engines.cuh"
+#include "batch.hpp"
 
 #include <cstring>
 #include <mutex>
@@ -558,6 +559,34 @@ public:
         if(st != ROCRAND_STATUS_SUCCESS)
             return st;
         return generate(data, n, Dist::POISSON, p);
+    }
+
+    rocrand_status batch_descriptor(uint32_t dist, double p0, double p1, void* data, size_t n,
+                                    BatchReq& r, cudaStream_t stream) override
+    {
+        if constexpr(kFam != Family::XORWOW && kFam != Family::MRG32K3A)
+        {
+            return ROCRAND_STATUS_TYPE_ERROR;
+        }
+        else
+        {
+            rocrand_status st = init();
+            if(st != ROCRAND_STATUS_SUCCESS)
+                return st;
+            r       = BatchReq{};
+            r.kind  = kFam == Family::XORWOW ? BK_XORWOW : BK_MRG32K3A;
+            r.arena = m_arena;
+            r.start = m_start;
+            st      = batch_set_dist(r, dist, p0, p1, stream);
+            if(st == ROCRAND_STATUS_SUCCESS)
+                st = batch_layout(r, data, n);
+            if(st != ROCRAND_STATUS_SUCCESS)
+                return st;
+            unsigned iw, ow;
+            batch_widths(r.kind, dist, iw, ow);
+            m_start = static_cast<uint32_t>((m_start + (n + ow - 1) / ow) % kE);
+            return ROCRAND_STATUS_SUCCESS;
+        }
     }
 
 private:
