@@ -36,8 +36,6 @@ const DeviceInfo& device_info()
     return cache[dev];
 }
 
-namespace rb200
-{
 rocrand_generator_base_type* make_generator(rocrand_rng_type t)
 {
     switch(t)
@@ -61,7 +59,6 @@ rocrand_generator_base_type* make_generator(rocrand_rng_type t)
         default: return nullptr;
     }
 }
-} // namespace rb200
 
 template<class Fn>
 static rocrand_status guarded(Fn&& fn)
