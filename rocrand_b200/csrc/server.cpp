@@ -1,0 +1,635 @@
+// server.cpp -- serving loop: continuous batching of generate requests on resident
+// generator states.
+//
+// A server owns generator handles (states resident on the device for their lifetime), an
+// output pool of a fixed budget, and a worker thread.  Requests are queued by submit();
+// the worker admits them in arrival order as output memory frees up, packs the admitted
+// ones into one batch (batch.hpp: one persistent launch over a descriptor table), and keeps
+// up to `streams` batches in flight, so requests arriving while others run start as soon
+// as a stream and memory are free.  A stateful handle (XORWOW, MRG32k3a) is in at most one
+// batch at a time and its next batch waits on the previous one's event; Philox and Sobol
+// handles keep their position on the host and may appear several times in one batch.
+// Each result equals the same call made alone on the handle's generator: descriptors are
+// taken in submission order from the generator's own state (batch_descriptor).
+// The plain mode runs the same admission and memory pool but issues one ordinary
+// generate call per request on one stream: the per-request baseline.
+#include "batch.hpp"
+#include "common.hpp"
+#include "generators.hpp"
+
+#include <rocrand_b200.h>
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace rb200
+{
+namespace
+{
+
+double now_s()
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// First-fit allocator over the output pool (offsets, 512-byte granules).
+class PoolAllocator
+{
+public:
+    void reset(size_t bytes)
+    {
+        m_free.clear();
+        m_free[0] = bytes;
+        m_used    = 0;
+    }
+    bool alloc(size_t bytes, size_t& off)
+    {
+        bytes = (bytes + 511) & ~size_t(511);
+        for(auto it = m_free.begin(); it != m_free.end(); ++it)
+        {
+            if(it->second < bytes)
+                continue;
+            off              = it->first;
+            const size_t rem = it->second - bytes;
+            m_free.erase(it);
+            if(rem)
+                m_free[off + bytes] = rem;
+            m_used += bytes;
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes)
+    {
+        bytes = (bytes + 511) & ~size_t(511);
+        m_used -= bytes;
+        auto next = m_free.lower_bound(off);
+        if(next != m_free.end() && off + bytes == next->first)
+        {
+            bytes += next->second;
+            next = m_free.erase(next);
+        }
+        if(next != m_free.begin())
+        {
+            auto prev = std::prev(next);
+            if(prev->first + prev->second == off)
+            {
+                prev->second += bytes;
+                return;
+            }
+        }
+        m_free[off] = bytes;
+    }
+    size_t used() const { return m_used; }
+
+private:
+    std::map<size_t, size_t> m_free;
+    size_t                   m_used = 0;
+};
+
+struct Request
+{
+    unsigned long long ticket;
+    uint32_t           handle;
+    uint32_t           dist;
+    double             p0, p1;
+    size_t             n, bytes;
+    size_t             off   = 0;
+    int                state = 0; // 0 queued, 1 in flight, 2 done, 3 failed
+    rocrand_status     status = ROCRAND_STATUS_SUCCESS;
+    double             t_submit = 0, t_done = 0;
+    bool               release_when_done = false;
+};
+
+struct Handle
+{
+    std::unique_ptr<rocrand_generator_base_type> gen;
+    bool                                         stateful    = false;
+    cudaEvent_t                                  last        = nullptr; // its last batch
+    bool                                         last_pending = false;
+};
+
+struct InFlight
+{
+    cudaEvent_t           done = nullptr;
+    int                   stream = 0;
+    std::vector<Request*> reqs;
+};
+
+} // namespace
+
+class Server
+{
+public:
+    Server(size_t budget, unsigned streams, int plain) : m_budget(budget), m_plain(plain != 0)
+    {
+        m_nstreams = plain ? 1u : std::max(1u, std::min(streams, 8u));
+    }
+
+    rocrand_status start()
+    {
+        if(cudaGetDevice(&m_device) != cudaSuccess)
+            return ROCRAND_STATUS_INTERNAL_ERROR;
+        if(cudaMalloc(&m_pool, m_budget) != cudaSuccess)
+        {
+            m_pool = nullptr;
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        }
+        m_alloc.reset(m_budget);
+        for(unsigned s = 0; s < m_nstreams; s++)
+        {
+            cudaStream_t st = nullptr;
+            if(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+                return ROCRAND_STATUS_INTERNAL_ERROR;
+            m_streams.push_back(st);
+            m_plans.emplace_back(new BatchPlan());
+        }
+        m_worker = std::thread([this] { loop(); });
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    ~Server()
+    {
+        {
+            std::lock_guard<std::mutex> lock(m_mu);
+            m_stop = true;
+        }
+        m_cv.notify_all();
+        if(m_worker.joinable())
+            m_worker.join();
+        cudaSetDevice(m_device);
+        for(auto s : m_streams)
+            cudaStreamSynchronize(s);
+        m_plans.clear();
+        for(auto s : m_streams)
+            cudaStreamDestroy(s);
+        for(auto& h : m_handles)
+            if(h.last)
+                cudaEventDestroy(h.last);
+        m_handles.clear();
+        cudaFree(m_pool);
+    }
+
+    rocrand_status add_generator(rocrand_rng_type type, unsigned long long seed, uint32_t& id)
+    {
+        std::unique_ptr<rocrand_generator_base_type> g(make_generator(type));
+        if(!g)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        const bool stateful = type == ROCRAND_RNG_PSEUDO_XORWOW || type == ROCRAND_RNG_PSEUDO_DEFAULT
+                              || type == ROCRAND_RNG_PSEUDO_MRG32K3A;
+        const bool ok = stateful || type == ROCRAND_RNG_PSEUDO_PHILOX4_32_10
+                        || type == ROCRAND_RNG_QUASI_SOBOL32 || type == ROCRAND_RNG_QUASI_DEFAULT;
+        if(!ok)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        rocrand_status st = g->set_seed(seed);
+        if(st == ROCRAND_STATUS_SUCCESS)
+            st = g->set_stream(m_streams[0]);
+        if(st == ROCRAND_STATUS_SUCCESS)
+            st = g->init(); // the resident state is seeded now, on the server's stream
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        if(cudaStreamSynchronize(m_streams[0]) != cudaSuccess)
+            return ROCRAND_STATUS_LAUNCH_FAILURE;
+        Handle h;
+        h.gen      = std::move(g);
+        h.stateful = stateful;
+        if(cudaEventCreateWithFlags(&h.last, cudaEventDisableTiming) != cudaSuccess)
+            return ROCRAND_STATUS_INTERNAL_ERROR;
+        std::lock_guard<std::mutex> lock(m_mu);
+        id = static_cast<uint32_t>(m_handles.size());
+        m_handles.push_back(std::move(h));
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    rocrand_status submit(uint32_t handle, uint32_t dist, double p0, double p1, size_t n,
+                          bool release_when_done, unsigned long long& ticket)
+    {
+        if(dist >= BD_COUNT)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        if(n == 0)
+            return ROCRAND_STATUS_OUT_OF_RANGE;
+        const size_t bytes = n * batch_elem_size(dist);
+        if(bytes > m_budget)
+            return ROCRAND_STATUS_OUT_OF_RANGE;
+        std::lock_guard<std::mutex> lock(m_mu);
+        if(handle >= m_handles.size())
+            return ROCRAND_STATUS_NOT_CREATED;
+        auto r               = std::make_unique<Request>();
+        r->ticket            = ++m_next_ticket;
+        r->handle            = handle;
+        r->dist              = dist;
+        r->p0                = p0;
+        r->p1                = p1;
+        r->n                 = n;
+        r->bytes             = bytes;
+        r->t_submit          = now_s();
+        r->release_when_done = release_when_done;
+        ticket               = r->ticket;
+        m_queue.push_back(r.get());
+        m_reqs[ticket] = std::move(r);
+        m_cv.notify_all();
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    rocrand_status wait(unsigned long long ticket, void** out, double* latency)
+    {
+        std::unique_lock<std::mutex> lock(m_mu);
+        auto                         it = m_reqs.find(ticket);
+        if(it == m_reqs.end())
+            return ROCRAND_STATUS_OUT_OF_RANGE;
+        Request* r = it->second.get();
+        m_done_cv.wait(lock, [&] { return r->state >= 2; });
+        if(out)
+            *out = r->release_when_done ? nullptr : m_pool + r->off;
+        if(latency)
+            *latency = r->t_done - r->t_submit;
+        return r->status;
+    }
+
+    rocrand_status release(unsigned long long ticket)
+    {
+        std::lock_guard<std::mutex> lock(m_mu);
+        auto                        it = m_reqs.find(ticket);
+        if(it == m_reqs.end())
+            return ROCRAND_STATUS_OUT_OF_RANGE;
+        Request* r = it->second.get();
+        if(r->state < 2)
+            return ROCRAND_STATUS_OUT_OF_RANGE; // still running
+        if(!r->release_when_done && r->state == 2)
+            m_alloc.release(r->off, r->bytes);
+        m_reqs.erase(it);
+        m_cv.notify_all();
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+private:
+    // Takes queued requests in arrival order while output memory lasts; a request that
+    // does not fit stops admission (no overtaking), a stateful handle joins a batch once.
+    void admit(std::vector<Request*>& out, size_t max_reqs, size_t max_bytes)
+    {
+        std::vector<uint32_t> used;
+        size_t                bytes = 0;
+        auto                  it    = m_queue.begin();
+        while(it != m_queue.end() && out.size() < max_reqs)
+        {
+            Request* r = *it;
+            const Handle& h = m_handles[r->handle];
+            if(h.stateful && std::find(used.begin(), used.end(), r->handle) != used.end())
+                break; // its next call must wait for this batch: keep arrival order
+            if(!out.empty() && bytes + r->bytes > max_bytes)
+                break;
+            size_t off = 0;
+            if(!m_alloc.alloc(r->bytes, off))
+                break;
+            r->off   = off;
+            r->state = 1;
+            bytes += r->bytes;
+            if(h.stateful)
+                used.push_back(r->handle);
+            out.push_back(r);
+            it = m_queue.erase(it);
+        }
+    }
+
+    void finish(Request* r, rocrand_status st)
+    {
+        r->status = st;
+        r->t_done = now_s();
+        r->state  = st == ROCRAND_STATUS_SUCCESS ? 2 : 3;
+        if(r->release_when_done || st != ROCRAND_STATUS_SUCCESS)
+            m_alloc.release(r->off, r->bytes);
+        if(r->release_when_done && st == ROCRAND_STATUS_SUCCESS)
+        {
+            // kept only for its latency until wait/release
+        }
+    }
+
+    // Launches one batch (or, in plain mode, one ordinary call) of admitted requests.
+    rocrand_status launch(std::vector<Request*>& reqs, int s)
+    {
+        cudaStream_t stream = m_streams[s];
+        if(m_plain)
+        {
+            Request* r = reqs[0];
+            Handle&  h = m_handles[r->handle];
+            h.gen->set_stream(stream);
+            void*          out = m_pool + r->off;
+            rocrand_status st;
+            DistParams     dp;
+            switch(r->dist)
+            {
+                case BD_UINT: st = h.gen->generate(out, r->n, Dist::U32, dp); break;
+                case BD_FLOAT: st = h.gen->generate(out, r->n, Dist::F32, dp); break;
+                case BD_DOUBLE: st = h.gen->generate(out, r->n, Dist::F64, dp); break;
+                case BD_NORMAL_F:
+                    dp.mean_f = static_cast<float>(r->p0);
+                    dp.std_f  = static_cast<float>(r->p1);
+                    st        = h.gen->generate(out, r->n, Dist::NORMAL_F32, dp);
+                    break;
+                default:
+                    st = h.gen->generate_poisson(static_cast<unsigned int*>(out), r->n, r->p0);
+                    break;
+            }
+            return st;
+        }
+        // each stream reuses its own descriptor table: its previous batch is finished
+        BatchPlan& plan = *m_plans[s];
+        plan.clear();
+        for(Request* r : reqs)
+        {
+            Handle&  h = m_handles[r->handle];
+            BatchReq d;
+            rocrand_status st
+                = h.gen->batch_descriptor(r->dist, r->p0, r->p1, m_pool + r->off, r->n, d, stream);
+            if(st != ROCRAND_STATUS_SUCCESS)
+                return st;
+            plan.add(d);
+            if(h.stateful && h.last_pending)
+                cudaStreamWaitEvent(stream, h.last, 0);
+        }
+        rocrand_status st = plan.upload(stream);
+        if(st == ROCRAND_STATUS_SUCCESS)
+            st = plan.launch(stream);
+        return st;
+    }
+
+    void loop()
+    {
+        cudaSetDevice(m_device);
+        std::deque<InFlight> inflight;
+        std::vector<bool>    busy(m_nstreams, false);
+        std::unique_lock<std::mutex> lock(m_mu);
+        for(;;)
+        {
+            // retire finished batches
+            bool retired = false;
+            for(auto it = inflight.begin(); it != inflight.end();)
+            {
+                if(cudaEventQuery(it->done) != cudaSuccess)
+                {
+                    ++it;
+                    continue;
+                }
+                for(Request* r : it->reqs)
+                    finish(r, ROCRAND_STATUS_SUCCESS);
+                busy[it->stream] = false;
+                cudaEventDestroy(it->done);
+                it      = inflight.erase(it);
+                retired = true;
+            }
+            if(retired)
+            {
+                for(auto& h : m_handles)
+                    if(h.last_pending && cudaEventQuery(h.last) == cudaSuccess)
+                        h.last_pending = false;
+                m_done_cv.notify_all();
+            }
+            if(m_stop && m_queue.empty() && inflight.empty())
+                return;
+            // start a batch on a free stream (plain calls: one stream, queued back to back)
+            int s = -1;
+            if(m_plain)
+                s = inflight.size() < kPlainInFlight ? 0 : -1;
+            else
+                for(unsigned k = 0; k < m_nstreams; k++)
+                    if(!busy[k])
+                    {
+                        s = static_cast<int>(k);
+                        break;
+                    }
+            if(s >= 0 && !m_queue.empty())
+            {
+                std::vector<Request*> reqs;
+                admit(reqs, m_plain ? 1 : 8192, m_plain ? m_budget : (size_t(8) << 30));
+                if(!reqs.empty())
+                {
+                    InFlight       f;
+                    f.stream          = s;
+                    rocrand_status st = launch(reqs, s);
+                    if(st != ROCRAND_STATUS_SUCCESS)
+                    {
+                        for(Request* r : reqs)
+                            finish(r, st);
+                        m_done_cv.notify_all();
+                        continue;
+                    }
+                    cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
+                    cudaEventRecord(f.done, m_streams[s]);
+                    if(!m_plain)
+                        for(Request* r : reqs)
+                        {
+                            Handle& h = m_handles[r->handle];
+                            if(h.stateful)
+                            {
+                                cudaEventRecord(h.last, m_streams[s]);
+                                h.last_pending = true;
+                            }
+                        }
+                    f.reqs = std::move(reqs);
+                    busy[s] = !m_plain;
+                    inflight.push_back(std::move(f));
+                    continue;
+                }
+            }
+            // nothing to start: poll the device again shortly, or sleep until a submit
+            if(inflight.empty())
+                m_cv.wait_for(lock, std::chrono::milliseconds(2));
+            else
+            {
+                lock.unlock();
+                std::this_thread::sleep_for(std::chrono::microseconds(5));
+                lock.lock();
+            }
+        }
+    }
+
+    static constexpr size_t       kPlainInFlight = 4096;
+    size_t                        m_budget;
+    bool                          m_plain;
+    unsigned                      m_nstreams = 1;
+    int                           m_device   = 0;
+    unsigned char*                m_pool     = nullptr;
+    PoolAllocator                 m_alloc;
+    std::vector<cudaStream_t>     m_streams;
+    std::vector<std::unique_ptr<BatchPlan>> m_plans;
+    std::vector<Handle>           m_handles;
+    std::deque<Request*>          m_queue;
+    std::unordered_map<unsigned long long, std::unique_ptr<Request>> m_reqs;
+    unsigned long long            m_next_ticket = 0;
+    std::mutex                    m_mu;
+    std::condition_variable       m_cv, m_done_cv;
+    std::thread                   m_worker;
+    bool                          m_stop = false;
+};
+
+} // namespace rb200
+
+using namespace rb200;
+
+struct rocrand_b200_server_st
+{
+    std::unique_ptr<Server> s;
+};
+
+extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_create(rocrand_b200_server* server,
+                                                                size_t output_budget,
+                                                                unsigned int streams, int plain_calls)
+{
+    if(server == nullptr || output_budget == 0)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    try
+    {
+        auto h = std::make_unique<rocrand_b200_server_st>();
+        h->s.reset(new Server(output_budget, streams, plain_calls));
+        const rocrand_status st = h->s->start();
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        *server = h.release();
+        return ROCRAND_STATUS_SUCCESS;
+    }
+    catch(...)
+    {
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+}
+
+extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_destroy(rocrand_b200_server server)
+{
+    if(server == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    delete server;
+    return ROCRAND_STATUS_SUCCESS;
+}
+
+extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_add_generator(rocrand_b200_server server,
+                                                                       rocrand_rng_type    rng_type,
+                                                                       unsigned long long  seed,
+                                                                       unsigned int*       handle)
+{
+    if(server == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    if(handle == nullptr)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    try
+    {
+        uint32_t             id = 0;
+        const rocrand_status st = server->s->add_generator(rng_type, seed, id);
+        *handle                 = id;
+        return st;
+    }
+    catch(...)
+    {
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+}
+
+extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_submit(rocrand_b200_server       server,
+                                                                unsigned int              handle,
+                                                                rocrand_b200_distribution distribution,
+                                                                double param0, double param1,
+                                                                size_t n, unsigned long long* ticket)
+{
+    if(server == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    if(ticket == nullptr)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    try
+    {
+        return server->s->submit(handle, static_cast<uint32_t>(distribution), param0, param1, n,
+                                 false, *ticket);
+    }
+    catch(...)
+    {
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+}
+
+extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_wait(rocrand_b200_server server,
+                                                              unsigned long long ticket, void** output,
+                                                              double* latency_seconds)
+{
+    if(server == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    try
+    {
+        return server->s->wait(ticket, output, latency_seconds);
+    }
+    catch(...)
+    {
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+}
+
+extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_release(rocrand_b200_server server,
+                                                                 unsigned long long  ticket)
+{
+    if(server == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    try
+    {
+        return server->s->release(ticket);
+    }
+    catch(...)
+    {
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+}
+
+extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_run_trace(rocrand_b200_server server,
+                                                                   const rocrand_b200_trace_item* items,
+                                                                   size_t count, double* latency_seconds,
+                                                                   double* wall_seconds)
+{
+    if(server == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    if(items == nullptr && count > 0)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    try
+    {
+        std::vector<unsigned long long> tickets(count);
+        const double                    t0 = now_s();
+        for(size_t i = 0; i < count; i++)
+        {
+            const double due = t0 + items[i].arrival_seconds;
+            while(now_s() < due)
+            {
+            }
+            const rocrand_status st
+                = server->s->submit(items[i].handle, static_cast<uint32_t>(items[i].distribution),
+                                    items[i].param0, items[i].param1, items[i].n, true, tickets[i]);
+            if(st != ROCRAND_STATUS_SUCCESS)
+                return st;
+        }
+        double last = t0;
+        for(size_t i = 0; i < count; i++)
+        {
+            double               lat = 0;
+            const rocrand_status st  = server->s->wait(tickets[i], nullptr, &lat);
+            if(st != ROCRAND_STATUS_SUCCESS)
+                return st;
+            if(latency_seconds)
+                latency_seconds[i] = lat;
+            last = std::max(last, t0 + items[i].arrival_seconds + lat);
+            server->s->release(tickets[i]);
+        }
+        if(wall_seconds)
+            *wall_seconds = last - t0;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+    catch(...)
+    {
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+}
