@@ -275,6 +275,14 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args.cpu_n, calls)
 
+    batched = serving = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        del out
+        torch.cuda.empty_cache()
+        batched = batched_leg(lib, args.full_configs)
+        torch.cuda.empty_cache()
+        serving = serving_leg(lib, args.full_configs)
+
     for g in gens.values():
         lib.rocrand_destroy_generator(g)
     if world > 1:
@@ -330,11 +338,179 @@ def run_ours(args):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if batched is not None:
+        line["batched_fill"] = batched
+    if serving is not None:
+        line["serving"] = serving
     print(json.dumps(line))
 
 
 # ------------------------------------------------------------------------------------
 # reference host generators (CPU)
+
+
+def splitmix64(i):
+    """SplitMix64 output for input i (Steele, Lea and Flood 2014; the mixing constants as
+    published by Vigna): the seeds of the batched-fill generators."""
+    m = (1 << 64) - 1
+    z = (i + 0x9E3779B97F4A7C15) & m
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    return z ^ (z >> 31)
+
+
+def _entry_args(d, p0, p1):
+    """(entry point, trailing arguments) of the plain call for batch distribution d."""
+    if d == 1:
+        return "rocrand_generate_uniform", []
+    if d == 3:
+        return "rocrand_generate_normal", [ctypes.c_float(p0), ctypes.c_float(p1)]
+    if d == 4:
+        return "rocrand_generate_poisson", [ctypes.c_double(p0)]
+    if d == 2:
+        return "rocrand_generate_uniform_double", []
+    return "rocrand_generate", []
+
+
+def batched_leg(lib, full):
+    """Config 4: 4096 Philox4x32-10 + 4096 XORWOW fresh generators (seed_i = splitmix64(i),
+    offset 0), sizes log-uniform in [2^10, 2^24] (numpy PCG64 seed 42), 50% uniform fp32 /
+    30% normal fp32 / 20% Poisson lambda=4; one persistent launch replayed from a CUDA graph
+    versus one plain call per generator (set_seed + generate, so every pass writes the same
+    values).  Without --full-configs a quarter of the requests (1024 + 1024)."""
+    import numpy as np
+    import torch
+    import rocrand_b200 as rb
+    per = 4096 if full else 1024
+    count = 2 * per
+    rs = np.random.Generator(np.random.PCG64(42))
+    sizes = np.exp(rs.uniform(np.log(2.0 ** 10), np.log(2.0 ** 24), count)).astype(np.int64)
+    u = rs.random(count)
+    dists = np.where(u < 0.5, 1, np.where(u < 0.8, 3, 4))
+    types = [rb.ROCRAND_RNG_PSEUDO_PHILOX4_32_10] * per + [rb.ROCRAND_RNG_PSEUDO_XORWOW] * per
+    seeds = [splitmix64(i) for i in range(count)]
+    offs, total = [], 0
+    for n in sizes:
+        offs.append(total)
+        total += (int(n) * 4 + 511) // 512 * 512
+    out = torch.zeros(total, dtype=torch.uint8, device="cuda")
+    base = out.data_ptr()
+    stream = torch.cuda.current_stream()
+    reqs = (rb.BatchRequest * count)()
+    params = {1: (0.0, 0.0), 3: (0.0, 1.0), 4: (4.0, 0.0)}
+    for k in range(count):
+        p0, p1 = params[int(dists[k])]
+        reqs[k] = rb.BatchRequest(types[k], int(dists[k]), seeds[k], 0, p0, p1, base + offs[k], int(sizes[k]))
+    byte_count = int(sizes.sum()) * 4
+
+    def checksum():
+        torch.cuda.synchronize()
+        return (int(out.view(torch.int64).sum().item()), int(out.view(torch.int32).sum(dtype=torch.int64).item()))
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # plain: one generator per request, re-seeded every pass (the XORWOW arena re-initialises)
+    gens = []
+    for k in range(count):
+        g = ctypes.c_void_p()
+        rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), types[k]))
+        rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
+        gens.append(g)
+    calls = [(gens[k], seeds[k], getattr(lib, _entry_args(int(dists[k]), *params[int(dists[k])])[0]),
+              c_void_p(base + offs[k]), c_size_t(int(sizes[k])),
+              _entry_args(int(dists[k]), *params[int(dists[k])])[1]) for k in range(count)]
+
+    def plain_pass():
+        for g, seed, fn, ptr, n, extra in calls:
+            lib.rocrand_set_seed(g, seed)
+            fn(g, ptr, n, *extra)
+
+    plain_ms = timed(plain_pass, 2)
+    plain_sum = checksum()
+    out.zero_()
+    rb.check_rocrand(lib.rocrand_b200_autotune_batch(c_void_p(stream.cuda_stream)))
+    plan = c_void_p()
+    rb.check_rocrand(lib.rocrand_b200_create_batch_plan(ctypes.byref(plan), reqs, count,
+                                                        c_void_p(stream.cuda_stream)))
+    batch_ms = timed(lambda: lib.rocrand_b200_execute_batch_plan(plan, 1, c_void_p(stream.cuda_stream)), 5)
+    batch_sum = checksum()
+    lib.rocrand_b200_destroy_batch_plan(plan)
+    for g in gens:
+        lib.rocrand_destroy_generator(g)
+    del out
+    return {"requests": count, "bytes_per_pass": byte_count,
+            "batched_gbs": round(byte_count / (batch_ms * 1e-3) / 1e9, 1),
+            "plain_gbs": round(byte_count / (plain_ms * 1e-3) / 1e9, 1),
+            "speedup": round(plain_ms / batch_ms, 2), "batched_ms": round(batch_ms, 3),
+            "plain_ms": round(plain_ms, 3), "identical_outputs": plain_sum == batch_sum,
+            "graph_replay": True, "autotuned": True,
+            "sizes": "log-uniform [2^10, 2^24], PCG64 seed 42",
+            "mix": "50% uniform fp32 / 30% normal fp32 / 20% Poisson 4"}
+
+
+def serving_leg(lib, full):
+    """Config 5: Poisson arrivals at 1k-50k req/s over 64 handles (16 each of Philox,
+    XORWOW, MRG32k3a, Sobol32; states resident), sizes log-uniform in [2^8, 2^26], dtypes
+    uniform over fp32 / fp64 / uint32, a 64 GB output budget; the continuous-batching server
+    and the plain per-request server replay the same trace.  Also a saturated trace (every
+    request at t=0).  Requests per rate: 10^5 with --full-configs, else 2000."""
+    import numpy as np
+    import rocrand_b200 as rb
+    types = [rb.ROCRAND_RNG_PSEUDO_PHILOX4_32_10, rb.ROCRAND_RNG_PSEUDO_XORWOW,
+             rb.ROCRAND_RNG_PSEUDO_MRG32K3A, rb.ROCRAND_RNG_QUASI_SOBOL32]
+    nreq = 100000 if full else 2000
+    budget = 64 << 30
+    rates = [1000, 5000, 10000, 20000, 50000, None]
+    results = {}
+    for mode in ("batched", "plain"):
+        server = c_void_p()
+        rb.check_rocrand(lib.rocrand_b200_server_create(ctypes.byref(server), budget, 3,
+                                                        1 if mode == "plain" else 0))
+        handles = []
+        for t in types:
+            for k in range(16):
+                h = ctypes.c_uint()
+                rb.check_rocrand(lib.rocrand_b200_server_add_generator(server, t, splitmix64(len(handles)),
+                                                                       ctypes.byref(h)))
+                handles.append(h.value)
+        for rate in rates:
+            rs = np.random.Generator(np.random.PCG64(7))
+            n = nreq if rate is None or rate >= 5000 or full else min(nreq, 1000)
+            gaps = rs.exponential(1.0 / rate, n) if rate else np.zeros(n)
+            arrivals = np.cumsum(gaps) if rate else gaps
+            hidx = rs.integers(0, len(handles), n)
+            dts = rs.integers(0, 3, n)  # uint32, fp32, fp64
+            sizes = np.exp(rs.uniform(np.log(2.0 ** 8), np.log(2.0 ** 26), n)).astype(np.int64)
+            items = (rb.TraceItem * n)()
+            dist_of = {0: 0, 1: 1, 2: 2}
+            nbytes = 0
+            for i in range(n):
+                items[i] = rb.TraceItem(float(arrivals[i]), handles[hidx[i]], dist_of[int(dts[i])], 0.0, 0.0,
+                                        int(sizes[i]))
+                nbytes += int(sizes[i]) * (8 if dts[i] == 2 else 4)
+            lat = (ctypes.c_double * n)()
+            wall = ctypes.c_double()
+            rb.check_rocrand(lib.rocrand_b200_server_run_trace(server, items, n, lat, ctypes.byref(wall)))
+            l = np.ctypeslib.as_array(lat)
+            key = "saturated" if rate is None else "%d_req_s" % rate
+            results.setdefault(key, {"requests": n})[mode] = {
+                "gbs": round(nbytes / wall.value / 1e9, 1), "p50_ms": round(float(np.percentile(l, 50)) * 1e3, 3),
+                "p99_ms": round(float(np.percentile(l, 99)) * 1e3, 3), "wall_s": round(wall.value, 3)}
+        rb.check_rocrand(lib.rocrand_b200_server_destroy(server))
+    for v in results.values():
+        if "batched" in v and "plain" in v:
+            v["gbs_ratio"] = round(v["batched"]["gbs"] / v["plain"]["gbs"], 2)
+    return {"budget_bytes": budget, "handles": 64, "streams": 3,
+            "sizes": "log-uniform [2^8, 2^26]", "dtypes": "uint32/fp32/fp64", "rates": results}
 
 
 def _ref_lib():
@@ -469,6 +645,9 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=1 << 24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="", help="gen:dist[:param],... subset of the sweep")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-fill and serving legs")
+    ap.add_argument("--full-configs", action="store_true",
+                    help="batched fill with 4096+4096 generators, serving with 10^5 requests per rate")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -70,7 +70,39 @@ ROCRAND_STATUS = {
 
 # (name, argtypes) of every exported function; the half parameters travel as their 16 bits.
 _G = c_void_p
+class BatchRequest(ctypes.Structure):
+    """rocrand_b200_request (include/rocrand_b200.h): one plain call of a batched fill."""
+    _fields_ = [("rng_type", c_int), ("distribution", c_int), ("seed", ctypes.c_ulonglong),
+                ("offset", ctypes.c_ulonglong), ("param0", ctypes.c_double),
+                ("param1", ctypes.c_double), ("output", c_void_p), ("n", c_size_t)]
+
+
+class TraceItem(ctypes.Structure):
+    """rocrand_b200_trace_item (include/rocrand_b200.h): one timed request of a trace."""
+    _fields_ = [("arrival_seconds", ctypes.c_double), ("handle", ctypes.c_uint),
+                ("distribution", c_int), ("param0", ctypes.c_double),
+                ("param1", ctypes.c_double), ("n", c_size_t)]
+
+
+# batch distributions of rocrand_b200_request
+B200_DIST_UINT, B200_DIST_UNIFORM_FLOAT, B200_DIST_UNIFORM_DOUBLE, B200_DIST_NORMAL_FLOAT, \
+    B200_DIST_POISSON = range(5)
+
 _SIGNATURES = [
+    ("rocrand_b200_generate_batch", [c_void_p, c_size_t, c_void_p]),
+    ("rocrand_b200_create_batch_plan", [POINTER(c_void_p), c_void_p, c_size_t, c_void_p]),
+    ("rocrand_b200_execute_batch_plan", [c_void_p, c_int, c_void_p]),
+    ("rocrand_b200_destroy_batch_plan", [c_void_p]),
+    ("rocrand_b200_autotune_batch", [c_void_p]),
+    ("rocrand_b200_get_batch_tile", [c_int, c_int, c_void_p]),
+    ("rocrand_b200_server_create", [POINTER(c_void_p), c_size_t, ctypes.c_uint, c_int]),
+    ("rocrand_b200_server_destroy", [c_void_p]),
+    ("rocrand_b200_server_add_generator", [c_void_p, c_int, ctypes.c_ulonglong, c_void_p]),
+    ("rocrand_b200_server_submit", [c_void_p, ctypes.c_uint, c_int, ctypes.c_double, ctypes.c_double,
+                                    c_size_t, c_void_p]),
+    ("rocrand_b200_server_wait", [c_void_p, ctypes.c_ulonglong, c_void_p, c_void_p]),
+    ("rocrand_b200_server_release", [c_void_p, ctypes.c_ulonglong]),
+    ("rocrand_b200_server_run_trace", [c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
     ("rocrand_create_generator", [POINTER(c_void_p), c_int]),
     ("rocrand_create_generator_host", [POINTER(c_void_p), c_int]),
     ("rocrand_create_generator_host_blocking", [POINTER(c_void_p), c_int]),

@@ -54,6 +54,7 @@ struct BatchLaunch
     unsigned long long  tiles;
     unsigned long long* next;
     const uint32_t*     xorwow_tables;
+    const uint32_t*     xorwow_lanes;
     const uint64_t*     mrg_tables;
 };
 
@@ -141,25 +142,28 @@ __device__ __forceinline__ void philox_tile(const BatchReq& r, unsigned long lon
 }
 
 // Engine e of a fresh generator: the base state of its side of `start`, jumped e
-// subsequences with the per-digit tables (as the plain generator's init kernels do).
+// subsequences (as the plain generator's init kernels do).  XORWOW seeds warp-cooperatively:
+// every lane of the warp must call this together.
 template<class E>
-__device__ __forceinline__ void seed_engine(const BatchReq& r, uint32_t e, E& eng,
-                                            const uint32_t* xt, const uint64_t* mt)
+__device__ __forceinline__ void seed_engine(const BatchReq& r, uint32_t e, E& eng, const BatchLaunch& L)
 {
     const int which = e < r.start ? 1 : 0;
 #pragma unroll
     for(int k = 0; k < 6; k++)
         eng.w[k] = r.base[which][k];
-    for(int p = 0; p < kJumpDigits; p++)
+    if constexpr(std::is_same_v<E, XorwowEngine>)
     {
-        const uint32_t d = (e >> (2 * p)) & 3u;
-        if(!d)
-            continue;
-        if constexpr(std::is_same_v<E, XorwowEngine>)
-            gf2_apply<5>(xt + (static_cast<size_t>(p) * 3 + (d - 1)) * (5 * 32 * 5), eng.w);
-        else
+        const bool shared = which == __shfl_sync(0xffffffffu, which, 0);
+        xorwow_seed(eng.w, e, L.xorwow_tables, L.xorwow_lanes, shared);
+    }
+    else
+    {
+        for(int p = 0; p < kJumpDigits; p++)
         {
-            const uint64_t* t = mt + ((static_cast<size_t>(p) * 3 + (d - 1)) * 2) * 9;
+            const uint32_t d = (e >> (2 * p)) & 3u;
+            if(!d)
+                continue;
+            const uint64_t* t = L.mrg_tables + ((static_cast<size_t>(p) * 3 + (d - 1)) * 2) * 9;
             mod_apply(t, 4294967087ull, eng.w);
             mod_apply(t + 9, 4294944443ull, eng.w + 3);
         }
@@ -177,23 +181,28 @@ __device__ __forceinline__ void stateful_tile(const BatchReq& r, unsigned long l
     const unsigned long long need = r.vec_n >= kBatchE ? kBatchE : r.vec_n + (has_edge ? 1 : 0);
     const unsigned long long t0   = local * r.units;
     const unsigned long long t1   = t0 + r.units < need ? t0 + r.units : need;
-    for(unsigned long long t = t0 + threadIdx.x; t < t1; t += blockDim.x)
+    // the whole block steps together (seeding is warp-cooperative); lanes past t1 or without
+    // a vector of this call seed and then skip
+    for(unsigned long long tb = t0; tb < t1; tb += blockDim.x)
     {
-        const bool loops = t < r.vec_n;
-        const bool edges = has_edge && edge_slot == t;
-        if(!loops && !edges)
-            continue;
-        const uint32_t e = static_cast<uint32_t>((t + r.start) & (kBatchE - 1));
-        E              eng;
+        const unsigned long long t     = tb + threadIdx.x;
+        const bool               loops = t < t1 && t < r.vec_n;
+        const bool               edges = t < t1 && has_edge && edge_slot == t;
+        const uint32_t           e     = static_cast<uint32_t>((t + r.start) & (kBatchE - 1));
+        E                        eng;
         if(r.arena)
         {
+            if(!loops && !edges)
+                continue;
 #pragma unroll
             for(int k = 0; k < E::kWords; k++)
                 eng.w[k] = r.arena[static_cast<size_t>(k) * kBatchE + e];
         }
         else
         {
-            seed_engine(r, e, eng, L.xorwow_tables, L.mrg_tables);
+            seed_engine(r, e, eng, L);
+            if(!loops && !edges)
+                continue;
         }
         uint32_t           in[F::iw];
         T                  out[F::ow];
@@ -632,8 +641,9 @@ rocrand_status BatchPlan::launch(cudaStream_t stream)
     L.tiles         = m_tiles;
     L.next          = d_next;
     L.xorwow_tables = static_cast<const uint32_t*>(stateful_digit_tables(StatefulFamily::XORWOW));
+    L.xorwow_lanes  = stateful_xorwow_lane_tables();
     L.mrg_tables    = static_cast<const uint64_t*>(stateful_digit_tables(StatefulFamily::MRG32K3A));
-    if(L.xorwow_tables == nullptr || L.mrg_tables == nullptr)
+    if(L.xorwow_tables == nullptr || L.xorwow_lanes == nullptr || L.mrg_tables == nullptr)
         return ROCRAND_STATUS_ALLOCATION_FAILED;
     const unsigned long long want = m_tiles;
     unsigned                 grid = batch_grid();
@@ -652,6 +662,7 @@ rocrand_status BatchPlan::replay(cudaStream_t stream)
         // tables and the grid are resolved before capture (their first use uploads/queries)
         (void)batch_grid();
         if(stateful_digit_tables(StatefulFamily::XORWOW) == nullptr
+           || stateful_xorwow_lane_tables() == nullptr
            || stateful_digit_tables(StatefulFamily::MRG32K3A) == nullptr)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
         cudaStream_t cap = nullptr;

@@ -76,6 +76,8 @@ struct StatefulBases
 StatefulBases stateful_bases(StatefulFamily fam, unsigned long long seed, unsigned long long offset);
 // Per-digit subsequence jump tables of a family on the current device (uploaded once).
 const void* stateful_digit_tables(StatefulFamily fam);
+// XORWOW lane tables J^r, r < 64, of the warp-cooperative seeding (uploaded once).
+const uint32_t* stateful_xorwow_lane_tables();
 
 // Generator of any type (api.cpp); nullptr for an unknown type.
 rocrand_generator_base_type* make_generator(rocrand_rng_type t);

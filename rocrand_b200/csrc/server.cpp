@@ -92,17 +92,18 @@ public:
         }
         m_free[off] = bytes;
     }
-    size_t used() const { return m_used; }
-
 private:
     std::map<size_t, size_t> m_free;
     size_t                   m_used = 0;
 };
 
+struct Handle;
+
 struct Request
 {
     unsigned long long ticket;
     uint32_t           handle;
+    Handle*            h = nullptr; // stable: handles live in a deque
     uint32_t           dist;
     double             p0, p1;
     size_t             n, bytes;
@@ -213,8 +214,10 @@ public:
         return ROCRAND_STATUS_SUCCESS;
     }
 
+    // t_arrival: when the request arrived (steady clock seconds), 0 = now; latency is
+    // measured from it, so time a late submitter spends is queueing latency too.
     rocrand_status submit(uint32_t handle, uint32_t dist, double p0, double p1, size_t n,
-                          bool release_when_done, unsigned long long& ticket)
+                          bool release_when_done, double t_arrival, unsigned long long& ticket)
     {
         if(dist >= BD_COUNT)
             return ROCRAND_STATUS_TYPE_ERROR;
@@ -229,12 +232,13 @@ public:
         auto r               = std::make_unique<Request>();
         r->ticket            = ++m_next_ticket;
         r->handle            = handle;
+        r->h                 = &m_handles[handle];
         r->dist              = dist;
         r->p0                = p0;
         r->p1                = p1;
         r->n                 = n;
         r->bytes             = bytes;
-        r->t_submit          = now_s();
+        r->t_submit          = t_arrival > 0 ? t_arrival : now_s();
         r->release_when_done = release_when_done;
         ticket               = r->ticket;
         m_queue.push_back(r.get());
@@ -279,15 +283,26 @@ private:
     // does not fit stops admission (no overtaking), a stateful handle joins a batch once.
     void admit(std::vector<Request*>& out, size_t max_reqs, size_t max_bytes)
     {
-        std::vector<uint32_t> used;
+        std::vector<uint32_t> used, blocked;
         size_t                bytes = 0;
         auto                  it    = m_queue.begin();
+        auto has = [](const std::vector<uint32_t>& v, uint32_t x) {
+            return std::find(v.begin(), v.end(), x) != v.end();
+        };
         while(it != m_queue.end() && out.size() < max_reqs)
         {
-            Request* r = *it;
-            const Handle& h = m_handles[r->handle];
-            if(h.stateful && std::find(used.begin(), used.end(), r->handle) != used.end())
-                break; // its next call must wait for this batch: keep arrival order
+            Request*      r = *it;
+            const Handle& h = *r->h;
+            // a stateful handle joins a batch once; its later requests (and anything after a
+            // skipped request of the same handle) wait for the next batch, so each handle
+            // keeps its arrival order while other handles' requests go ahead
+            if(has(blocked, r->handle) || (h.stateful && has(used, r->handle)))
+            {
+                if(!has(blocked, r->handle))
+                    blocked.push_back(r->handle);
+                ++it;
+                continue;
+            }
             if(!out.empty() && bytes + r->bytes > max_bytes)
                 break;
             size_t off = 0;
@@ -323,7 +338,7 @@ private:
         if(m_plain)
         {
             Request* r = reqs[0];
-            Handle&  h = m_handles[r->handle];
+            Handle&  h = *r->h;
             h.gen->set_stream(stream);
             void*          out = m_pool + r->off;
             rocrand_status st;
@@ -349,7 +364,7 @@ private:
         plan.clear();
         for(Request* r : reqs)
         {
-            Handle&  h = m_handles[r->handle];
+            Handle&  h = *r->h;
             BatchReq d;
             rocrand_status st
                 = h.gen->batch_descriptor(r->dist, r->p0, r->p1, m_pool + r->off, r->n, d, stream);
@@ -415,9 +430,13 @@ private:
                 admit(reqs, m_plain ? 1 : 8192, m_plain ? m_budget : (size_t(8) << 30));
                 if(!reqs.empty())
                 {
-                    InFlight       f;
-                    f.stream          = s;
+                    InFlight f;
+                    f.stream = s;
+                    // admitted requests, their handles and the streams belong to this thread:
+                    // launch without holding the queue lock, so submitters are not delayed
+                    lock.unlock();
                     rocrand_status st = launch(reqs, s);
+                    lock.lock();
                     if(st != ROCRAND_STATUS_SUCCESS)
                     {
                         for(Request* r : reqs)
@@ -430,7 +449,7 @@ private:
                     if(!m_plain)
                         for(Request* r : reqs)
                         {
-                            Handle& h = m_handles[r->handle];
+                            Handle& h = *r->h;
                             if(h.stateful)
                             {
                                 cudaEventRecord(h.last, m_streams[s]);
@@ -464,7 +483,7 @@ private:
     PoolAllocator                 m_alloc;
     std::vector<cudaStream_t>     m_streams;
     std::vector<std::unique_ptr<BatchPlan>> m_plans;
-    std::vector<Handle>           m_handles;
+    std::deque<Handle>            m_handles;
     std::deque<Request*>          m_queue;
     std::unordered_map<unsigned long long, std::unique_ptr<Request>> m_reqs;
     unsigned long long            m_next_ticket = 0;
@@ -548,7 +567,7 @@ extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_submit(rocrand_b200_ser
     try
     {
         return server->s->submit(handle, static_cast<uint32_t>(distribution), param0, param1, n,
-                                 false, *ticket);
+                                 false, 0.0, *ticket);
     }
     catch(...)
     {
@@ -608,11 +627,11 @@ extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_run_trace(rocrand_b200_
             }
             const rocrand_status st
                 = server->s->submit(items[i].handle, static_cast<uint32_t>(items[i].distribution),
-                                    items[i].param0, items[i].param1, items[i].n, true, tickets[i]);
+                                    items[i].param0, items[i].param1, items[i].n, true, due,
+                                    tickets[i]);
             if(st != ROCRAND_STATUS_SUCCESS)
                 return st;
         }
-        double last = t0;
         for(size_t i = 0; i < count; i++)
         {
             double               lat = 0;
@@ -621,11 +640,11 @@ extern "C" rocrand_status ROCRANDAPI rocrand_b200_server_run_trace(rocrand_b200_
                 return st;
             if(latency_seconds)
                 latency_seconds[i] = lat;
-            last = std::max(last, t0 + items[i].arrival_seconds + lat);
             server->s->release(tickets[i]);
         }
+        // every request is complete once the last wait returns
         if(wall_seconds)
-            *wall_seconds = last - t0;
+            *wall_seconds = now_s() - t0;
         return ROCRAND_STATUS_SUCCESS;
     }
     catch(...)

@@ -68,6 +68,23 @@ __global__ void __launch_bounds__(kBlock) init_gf2(InitArgs a, const uint32_t* _
         a.arena[static_cast<size_t>(k) * kE + e] = x[k];
 }
 
+// XORWOW engines: warp-cooperative seeding (stateful_engines.cuh:xorwow_seed).
+__global__ void __launch_bounds__(kBlock)
+    init_xorwow(InitArgs a, const uint32_t* __restrict__ tables, const uint32_t* __restrict__ lanes)
+{
+    const uint32_t e     = blockIdx.x * kBlock + threadIdx.x; // kE is a multiple of the block
+    const int      which = e < a.start ? 1 : 0;
+    uint32_t       x[6];
+#pragma unroll
+    for(int k = 0; k < 6; k++)
+        x[k] = a.base[which][k];
+    const bool shared = which == __shfl_sync(0xffffffffu, which, 0);
+    xorwow_seed(x, e, tables, lanes, shared);
+#pragma unroll
+    for(int k = 0; k < 6; k++)
+        a.arena[static_cast<size_t>(k) * kE + e] = x[k];
+}
+
 // MRG engines: two 3-word components modulo m1 and m2.
 __global__ void __launch_bounds__(kBlock)
     init_mrg(InitArgs a, const uint64_t* __restrict__ tables, uint64_t m1, uint64_t m2)
@@ -207,6 +224,38 @@ static const void* digit_tables(Family fam)
         return nullptr;
     c.ptr[dev] = d;
     return d;
+}
+
+// XORWOW lane tables: J^r, r = 0..63, laid out [input bit][word][r] (one upload per device).
+static const uint32_t* xorwow_lane_tables()
+{
+    static DeviceTables c;
+    const int           dev = device_info().device;
+    std::lock_guard<std::mutex> lock(c.mu);
+    if(c.ptr[dev])
+        return static_cast<const uint32_t*>(c.ptr[dev]);
+    const Gf2Matrix       j   = gf2_pow2(xorwow_step_matrix(), 67);
+    Gf2Matrix             acc = Gf2Matrix::identity(5);
+    std::vector<uint32_t> t(static_cast<size_t>(160) * 5 * kXorwowLaneJumps);
+    for(uint32_t r = 0; r < kXorwowLaneJumps; r++)
+    {
+        for(size_t i = 0; i < 160; i++)
+            for(size_t k = 0; k < 5; k++)
+                t[(i * 5 + k) * kXorwowLaneJumps + r] = acc.rows[i * 5 + k];
+        acc = acc.then(j);
+    }
+    void* d = nullptr;
+    if(cudaMalloc(&d, t.size() * 4) != cudaSuccess)
+        return nullptr;
+    if(cudaMemcpy(d, t.data(), t.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        return nullptr;
+    c.ptr[dev] = d;
+    return static_cast<const uint32_t*>(d);
+}
+
+const uint32_t* stateful_xorwow_lane_tables()
+{
+    return xorwow_lane_tables();
 }
 
 // A^(2^k), k = 0..63, of the one-step map (host offset jumps), computed once per family.
@@ -512,7 +561,12 @@ public:
             return ROCRAND_STATUS_ALLOCATION_FAILED;
         const unsigned blocks = kE / kBlock;
         if constexpr(kFam == Family::XORWOW)
-            init_gf2<5, 6><<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables));
+        {
+            const uint32_t* lanes = xorwow_lane_tables();
+            if(lanes == nullptr)
+                return ROCRAND_STATUS_ALLOCATION_FAILED;
+            init_xorwow<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables), lanes);
+        }
         else if constexpr(kFam == Family::LFSR113)
             init_gf2<4, 4><<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables));
         else if constexpr(kFam == Family::MRG32K3A)

@@ -156,6 +156,86 @@ __device__ __forceinline__ void mod_apply(const uint64_t* __restrict__ a, uint64
         x[r] = y[r];
 }
 
+// y = M x for one 160x160 GF(2) matrix (column-wise: column i = image of input bit i, 5
+// words at m + 5 i) and one x held identically by all 32 lanes of a warp: lane l folds the
+// columns of bits l, 32+l, ..., 128+l, then the partial results are XOR-reduced across the
+// warp.  25 loads and 25 shuffles per lane instead of 160 x 5 loads.
+__device__ __forceinline__ void gf2_apply_warp(const uint32_t* __restrict__ m, uint32_t* x)
+{
+    const uint32_t l = threadIdx.x & 31u;
+    uint32_t       y[5] = {0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+    for(int w = 0; w < 5; w++)
+    {
+        const uint32_t  mask = 0u - ((x[w] >> l) & 1u);
+        const uint32_t* col  = m + (32u * w + l) * 5u;
+#pragma unroll
+        for(int k = 0; k < 5; k++)
+            y[k] ^= mask & __ldg(col + k);
+    }
+#pragma unroll
+    for(int k = 0; k < 5; k++)
+    {
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            y[k] ^= __shfl_xor_sync(0xffffffffu, y[k], o);
+        x[k] = y[k];
+    }
+}
+
+// Lane tables of XORWOW seeding: J^r for r = 0..63 (J = one subsequence, 2^67 steps),
+// stored [input bit i][word k][r] so that a warp whose lanes apply different r reads
+// consecutive words.
+constexpr uint32_t kXorwowLaneJumps = 64;
+
+// The XORWOW engine e of a generator whose engines start from `x` (words 0..4 jumped, the
+// Weyl word 5 kept): x <- J^e x.  Must be called by all 32 lanes of the warp together
+// (it synchronises them).  e = 64 q + r: when the lanes share q and x (shared_base in every
+// lane), J^(64 q) is applied by the warp together (radix-4 digits 3..8) and J^r by each lane
+// from the lane table; otherwise each lane applies its own 9 digits.
+__device__ __forceinline__ void xorwow_seed(uint32_t* x, uint32_t e, const uint32_t* __restrict__ digits,
+                                            const uint32_t* __restrict__ lanes, bool shared_base)
+{
+    constexpr size_t msize = 5 * 32 * 5;
+    const uint32_t   q     = e >> 6;
+    const uint32_t   q0    = __shfl_sync(0xffffffffu, q, 0);
+    if(!__all_sync(0xffffffffu, shared_base && q == q0))
+    {
+        for(int p = 0; p < 9; p++)
+        {
+            const uint32_t d = (e >> (2 * p)) & 3u;
+            if(d)
+                gf2_apply<5>(digits + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
+        }
+        return;
+    }
+    for(int p = 3; p < 9; p++)
+    {
+        const uint32_t d = (q >> (2 * (p - 3))) & 3u; // the same in every lane
+        if(d)
+            gf2_apply_warp(digits + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
+    }
+    const uint32_t r = e & 63u;
+    uint32_t       y[5] = {0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+    for(int w = 0; w < 5; w++)
+    {
+        const uint32_t xw = x[w];
+#pragma unroll 4
+        for(int b = 0; b < 32; b++)
+        {
+            const uint32_t  mask = 0u - ((xw >> b) & 1u);
+            const uint32_t* row  = lanes + static_cast<size_t>((32 * w + b) * 5) * kXorwowLaneJumps + r;
+#pragma unroll
+            for(int k = 0; k < 5; k++)
+                y[k] ^= mask & __ldg(row + k * kXorwowLaneJumps);
+        }
+    }
+#pragma unroll
+    for(int k = 0; k < 5; k++)
+        x[k] = y[k];
+}
+
 template<class T, unsigned N>
 __device__ __forceinline__ void store_small(unsigned char* p, const T (&v)[N])
 {
