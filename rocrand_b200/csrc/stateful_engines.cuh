@@ -215,20 +215,21 @@ __device__ __forceinline__ void xorwow_seed(uint32_t* x, uint32_t e, const uint3
         if(d)
             gf2_apply_warp(digits + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
     }
+    // x is the same in every lane here, so the loop visits only its set bits, uniformly
     const uint32_t r = e & 63u;
     uint32_t       y[5] = {0u, 0u, 0u, 0u, 0u};
 #pragma unroll
     for(int w = 0; w < 5; w++)
     {
-        const uint32_t xw = x[w];
-#pragma unroll 4
-        for(int b = 0; b < 32; b++)
+        uint32_t bits = x[w];
+        while(bits)
         {
-            const uint32_t  mask = 0u - ((xw >> b) & 1u);
-            const uint32_t* row  = lanes + static_cast<size_t>((32 * w + b) * 5) * kXorwowLaneJumps + r;
+            const int       b   = __ffs(bits) - 1;
+            const uint32_t* row = lanes + static_cast<size_t>((32 * w + b) * 5) * kXorwowLaneJumps + r;
+            bits &= bits - 1;
 #pragma unroll
             for(int k = 0; k < 5; k++)
-                y[k] ^= mask & __ldg(row + k * kXorwowLaneJumps);
+                y[k] ^= __ldg(row + k * kXorwowLaneJumps);
         }
     }
 #pragma unroll
