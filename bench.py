@@ -14,9 +14,11 @@ cpu_baseline = the reference's own host generators (oracle/_ref, compiled from t
          sources) on this host's cores, on a bounded sample of the same sweep.
 
 --impl reference runs only the reference's CPU host generators on the same workload.
-Multi-GPU (torchrun): each rank fills its own disjoint slice of every stream (offset =
-rank * n), no data-path collective; weak scaling.  MT19937 has no offset: rank r uses seed
-0xdeadbeef + r (an independent stream of the same size).
+Multi-GPU (torchrun): each rank fills its own slice [r*n, (r+1)*n) of every stream by
+offset (rank_stream), no data-path collective; weak scaling.  Where an offset cannot select
+that slice -- MT19937 has no offset, and a stateful engine consuming two values per output
+maps offset and output positions differently -- rank r uses seed 0xdeadbeef + r instead
+(an independent stream of the same size).
 """
 
 import argparse
@@ -40,6 +42,18 @@ FALLBACK_HBM_GBS = 6650.0
 SWEEP_GENERATORS = [("philox4x32_10", 404), ("xorwow", 401), ("mrg32k3a", 402), ("lfsr113", 406),
                     ("mt19937", 407), ("threefry4x32_20", 410)]
 NO_OFFSET = {407}  # MT19937: set_offset is a TYPE_ERROR
+STATEFUL = {401, 402, 405, 406}
+TWO_WORD = {"uniform_double", "normal", "normal_double", "log_normal", "log_normal_double"}
+
+
+def rank_stream(gtype, dist, rank, n):
+    """(seed, offset or None) giving rank `rank` the outputs [rank*n, (rank+1)*n) of the
+    stream of seed SEED.  Counter engines, and stateful engines at one engine value per
+    output, continue the stream at an offset (out_offset[i] = out_0[offset + i]); MT19937
+    and two-value stateful distributions take seed SEED + rank instead."""
+    if gtype in NO_OFFSET or (gtype in STATEFUL and dist in TWO_WORD):
+        return SEED + rank, None
+    return SEED, stream_offset(dist, rank * n)
 SWEEP_DISTS = [
     ("uint", None), ("uniform", None), ("uniform_double", None), ("uniform_half", None),
     ("normal", (0.0, 1.0)), ("normal_double", (0.0, 1.0)), ("log_normal", (0.0, 1.0)),
@@ -193,11 +207,10 @@ def run_ours(args):
     for gname, gtype, d, p in calls:
         g = c_void_p()
         rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), gtype))
-        if gtype in NO_OFFSET:
-            rb.check_rocrand(lib.rocrand_set_seed(g, SEED + rank))
-        else:
-            rb.check_rocrand(lib.rocrand_set_seed(g, SEED))
-            rb.check_rocrand(lib.rocrand_set_offset(g, stream_offset(d, rank * n)))
+        seed, offset = rank_stream(gtype, d, rank, n)
+        rb.check_rocrand(lib.rocrand_set_seed(g, seed))
+        if offset is not None:
+            rb.check_rocrand(lib.rocrand_set_offset(g, offset))
         rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
         gens[(gname, d, p)] = g
 
