@@ -22,6 +22,7 @@ static int is_supported(int t)
         case ORC_RNG_MRG31K3P:
         case ORC_RNG_LFSR113:
         case ORC_RNG_MT19937:
+        case ORC_RNG_MTGP32:
         case ORC_RNG_SOBOL32:
         case ORC_RNG_SCRAMBLED_SOBOL32:
         case ORC_RNG_SOBOL64:
@@ -72,6 +73,7 @@ int orc_destroy(orc_gen* g)
         orc_poisson_free(&g->poisson);
         free(g->stf.engines);
         orc_mt19937_free(g);
+        orc_mtgp32_free(g);
         free(g);
     }
     return ORC_SUCCESS;
@@ -103,6 +105,13 @@ int orc_initialize(orc_gen* g)
         case ORC_RNG_MT19937:
         {
             const int st = orc_mt19937_init(g);
+            if(st != ORC_SUCCESS)
+                return st;
+            break;
+        }
+        case ORC_RNG_MTGP32:
+        {
+            const int st = orc_mtgp32_init(g);
             if(st != ORC_SUCCESS)
                 return st;
             break;
@@ -162,8 +171,8 @@ int orc_set_offset(orc_gen* g, unsigned long long offset)
 {
     if(!g)
         return ORC_NOT_CREATED;
-    if(g->rng_type == ORC_RNG_MT19937)
-        return ORC_TYPE_ERROR; /* mt19937.hpp:758-763 */
+    if(g->rng_type == ORC_RNG_MT19937 || g->rng_type == ORC_RNG_MTGP32)
+        return ORC_TYPE_ERROR; /* mt19937.hpp:758-763, mtgp32.hpp:389-393 */
     g->offset      = offset;
     g->initialized = 0;
     return ORC_SUCCESS;
@@ -272,6 +281,8 @@ static int run(orc_gen* g, void* data, size_t n, const orc_dist* din)
         return orc_threefry_generate(g, data, n, &d);
     if(g->rng_type == ORC_RNG_MT19937)
         return orc_mt19937_generate(g, data, n, &d);
+    if(g->rng_type == ORC_RNG_MTGP32)
+        return orc_mtgp32_generate(g, data, n, &d);
     return orc_stateful_generate(g, data, n, &d);
 }
 

@@ -177,6 +177,12 @@ int  orc_mt19937_init(struct orc_gen* g);
 void orc_mt19937_free(struct orc_gen* g);
 int  orc_mt19937_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
 
+/* MTGP32 (orc_mtgp32.c): 512 block generators with published parameter sets. */
+struct orc_mtgp;
+int  orc_mtgp32_init(struct orc_gen* g);
+void orc_mtgp32_free(struct orc_gen* g);
+int  orc_mtgp32_generate(struct orc_gen* g, void* data, size_t n, const orc_dist* d);
+
 struct orc_gen {
     int                rng_type;
     int                order;
@@ -189,6 +195,7 @@ struct orc_gen {
     uint32_t           sobol_offset; /* 32-bit point counter of the Sobol generators */
     orc_stateful       stf;
     struct orc_mt*     mt;
+    struct orc_mtgp*   mtgp;
     union {
         orc_philox   philox;
         orc_threefry threefry;

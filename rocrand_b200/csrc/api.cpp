@@ -51,6 +51,7 @@ rocrand_generator_base_type* make_generator(rocrand_rng_type t)
         case ROCRAND_RNG_PSEUDO_MRG31K3P:
         case ROCRAND_RNG_PSEUDO_LFSR113: return make_stateful(t);
         case ROCRAND_RNG_PSEUDO_MT19937: return make_mt19937();
+        case ROCRAND_RNG_PSEUDO_MTGP32: return make_mtgp32();
         case ROCRAND_RNG_QUASI_DEFAULT:
         case ROCRAND_RNG_QUASI_SOBOL32:
         case ROCRAND_RNG_QUASI_SCRAMBLED_SOBOL32:

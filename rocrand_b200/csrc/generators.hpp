@@ -86,6 +86,7 @@ rocrand_generator_base_type* make_generator(rocrand_rng_type t);
 rocrand_generator_base_type* make_threefry(rocrand_rng_type t);
 rocrand_generator_base_type* make_stateful(rocrand_rng_type t);
 rocrand_generator_base_type* make_mt19937();
+rocrand_generator_base_type* make_mtgp32();
 rocrand_generator_base_type* make_sobol(rocrand_rng_type t);
 
 } // namespace rb200

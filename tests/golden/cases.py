@@ -128,6 +128,10 @@ CASES = {
     "mrg32k3a": pseudo_cases(402, _SO_ST + [(0, 7)], _st_corner(402)),
     "mrg31k3p": pseudo_cases(405, _SO_ST, _st_corner(405)),
     "lfsr113": pseudo_cases(406, _SO_ST, _st_corner(406)),
+    "mtgp32": pseudo_cases(403, [(1234, None), (0xdeadbeefcafe, None)],
+                           [{"rng": 403, "seed": 5, "offset": None,
+                             "calls": [["uint", 131072 * 3 + 77, [], 0], ["normal", 1 + 131072 * 4 + 1, [0.0, 1.0], 1],
+                                       ["char", 3 + 256 * 4 * 7, [], 1], ["uniform_double", 256 * 512, [], 0]]}]),
     "mt19937": [{"rng": 407, "seed": 1234, "offset": None, "calls": _MT_CALLS},
                 {"rng": 407, "seed": 0xdeadbeefcafe, "offset": None,
                  "calls": _mt_check(_MT_CALLS[::-1])}],

@@ -98,6 +98,21 @@ def test_discrete_null_arguments(lib):
     assert lib.rocrand_destroy_discrete_distribution(None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
 
 
+def test_mtgp32_host_side_semantics(lib):
+    """MTGP32 (mtgp32.hpp:389-416): no offset, the four pseudo orderings, no 64-bit output."""
+    st, g = _create(lib, rb.ROCRAND_RNG_PSEUDO_MTGP32)
+    assert st == 0
+    try:
+        assert lib.rocrand_set_offset(g, 5) == rb.ROCRAND_STATUS_TYPE_ERROR
+        for o in (rb.ROCRAND_ORDERING_PSEUDO_SEEDED, rb.ROCRAND_ORDERING_QUASI_DEFAULT):
+            assert lib.rocrand_set_ordering(g, o) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+        for o in (100, 101, 103, 104):
+            assert lib.rocrand_set_ordering(g, o) == 0
+        assert lib.rocrand_generate_long_long(g, None, 10) == rb.ROCRAND_STATUS_TYPE_ERROR
+    finally:
+        assert lib.rocrand_destroy_generator(g) == 0
+
+
 def test_mt19937_host_side_semantics(lib):
     """MT19937 (mt19937.hpp:758-780, 1044-1060): no offset, orderings DEFAULT/BEST/LEGACY
     only, no 64-bit output; all refused before any device work."""

@@ -23,7 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 PSEUDO = {"philox": 404, "threefry2x32": 408, "threefry2x64": 409, "threefry4x32": 410,
           "threefry4x64": 411, "xorwow": 401, "mrg32k3a": 402, "mrg31k3p": 405, "lfsr113": 406,
-          "mt19937": 407}
+          "mt19937": 407, "mtgp32": 403}
+NO_OFFSET = {"mt19937", "mtgp32"}  # set_offset is a TYPE_ERROR
 WORD64 = {"threefry2x64", "threefry4x64"}
 STATEFUL = {"xorwow", "mrg32k3a", "mrg31k3p", "lfsr113"}
 
@@ -72,8 +73,8 @@ def test_random_sequences(lib, orc, name, dist, params):
     rng = np.random.default_rng(zlib.crc32(repr((name, dist, params)).encode()))
     seed = int(rng.integers(0, 2**63))
     offset = int(rng.integers(0, 2**20)) if rng.random() < 0.5 else 0
-    if name == "mt19937":
-        offset = None  # MT19937 has no offset (set_offset is a TYPE_ERROR)
+    if name in NO_OFFSET:
+        offset = None
     calls = []
     for n in (1 << 20, 3, int(rng.integers(1, 100000)), (1 << 18) + 5):
         calls.append((dist, n, params, int(rng.integers(0, 16))))
@@ -133,7 +134,7 @@ def test_full_size_against_oracle_and_continuity(lib, orc, name, dist):
     import torch
     n = 1 << 28
     params = [0.0, 1.0] if dist == "normal" else []
-    offset = None if name == "mt19937" else 0
+    offset = None if name in NO_OFFSET else 0
     g = gu.create(lib, PSEUDO[name], 0xdeadbeef, offset)
     st, big = gu.device_generate(lib, g, dist, n, params, 0)
     assert st == 0
