@@ -16,7 +16,7 @@ cpu_baseline = the reference's own host generators (oracle/_ref, compiled from t
 --impl reference runs only the reference's CPU host generators on the same workload.
 Multi-GPU (torchrun): each rank fills its own slice [r*n, (r+1)*n) of every stream by
 offset (rank_stream), no data-path collective; weak scaling.  Where an offset cannot select
-that slice -- MT19937 has no offset, and a stateful engine consuming two values per output
+that slice -- MT19937 and MTGP32 have no offset, and a stateful engine consuming two values per output
 maps offset and output positions differently -- rank r uses seed 0xdeadbeef + r instead
 (an independent stream of the same size).
 """
@@ -40,8 +40,9 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Generator families in the sweep (rocrand_rng_type values), in the order they were built.
 SWEEP_GENERATORS = [("philox4x32_10", 404), ("xorwow", 401), ("mrg32k3a", 402), ("lfsr113", 406),
-                    ("mt19937", 407), ("threefry4x32_20", 410)]
-NO_OFFSET = {407}  # MT19937: set_offset is a TYPE_ERROR
+                    ("mt19937", 407), ("threefry4x32_20", 410), ("mtgp32", 403)]
+NO_OFFSET = {407, 403}  # MT19937, MTGP32: set_offset is a TYPE_ERROR
+PORT_SEEDED = {407}  # host streams seeded by the C port (the reference's host seeding is slow)
 STATEFUL = {401, 402, 405, 406}
 TWO_WORD = {"uniform_double", "normal", "normal_double", "log_normal", "log_normal_double"}
 
@@ -49,8 +50,8 @@ TWO_WORD = {"uniform_double", "normal", "normal_double", "log_normal", "log_norm
 def rank_stream(gtype, dist, rank, n):
     """(seed, offset or None) giving rank `rank` the outputs [rank*n, (rank+1)*n) of the
     stream of seed SEED.  Counter engines, and stateful engines at one engine value per
-    output, continue the stream at an offset (out_offset[i] = out_0[offset + i]); MT19937
-    and two-value stateful distributions take seed SEED + rank instead."""
+    output, continue the stream at an offset (out_offset[i] = out_0[offset + i]); MT19937,
+    MTGP32 and two-value stateful distributions take seed SEED + rank instead."""
     if gtype in NO_OFFSET or (gtype in STATEFUL and dist in TWO_WORD):
         return SEED + rank, None
     return SEED, stream_offset(dist, rank * n)
@@ -533,15 +534,15 @@ def _ref_lib():
     return pyorc.CLib("orc"), "port"
 
 
-_SEEDED = {}  # MT19937 host streams, seeded once per process
+_SEEDED = {}  # MT19937 / MTGP32 host streams, seeded once per process
 
 
 def cpu_sample(n_per_call, calls, threads):
     """Runs every call of the sweep on the reference's host generators, n_per_call values
     each, split over `threads` host threads (each its own generator, offset to its slice).
-    MT19937 has no offset, so each thread runs its own seed; and because the reference's host
-    MT19937 spends minutes seeding its 8192 generators, those are the C port's (lazily
-    seeded, warmed untimed).  Returns (bytes, seconds, kind)."""
+    MT19937 and MTGP32 have no offset, so each thread runs its own seed (seeded and warmed
+    untimed); because the reference's host MT19937 spends minutes seeding its 8192
+    generators, those are the C port's.  Returns (bytes, seconds, kind)."""
     import numpy as np
     from concurrent.futures import ThreadPoolExecutor
     from oracle import pyorc
@@ -549,7 +550,7 @@ def cpu_sample(n_per_call, calls, threads):
     total_bytes = 0
     t_all = 0.0
     for gname, gtype, d, p in calls:
-        lib = pyorc.CLib("orc") if gtype in NO_OFFSET else ref_lib
+        lib = pyorc.CLib("orc") if gtype in PORT_SEEDED else ref_lib
         suffix, dt, _ = pyorc.DISTS[d]
         buf = np.empty(n_per_call + 64, dtype=dt)
         base = (-buf.ctypes.data // buf.itemsize) % (64 // buf.itemsize)
@@ -572,8 +573,8 @@ def cpu_sample(n_per_call, calls, threads):
                     lib.set_offset(g, stream_offset(d, a))
                 gens.append(g)
         if gtype in NO_OFFSET and key not in _SEEDED:
-            # untimed, once per stream: a call of >= 65536 units seeds all 8192 generators;
-            # later samples continue the same streams
+            # untimed, once per stream: a call of >= 65536 units seeds all 8192 MT19937
+            # generators; later samples continue the same streams
             warm = [np.empty(1 << 18, dtype=dt) for _ in range(threads)]
 
             def seed_all(i):
@@ -605,8 +606,8 @@ def cpu_baseline_sample(n_per_call, calls):
     nb, secs, kind = cpu_sample(n_per_call, calls, threads)
     return {"value": round(nb / secs / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
             "sample": "same sweep at n=%d values per call (vs 2^28 on the GPU), %d host threads, "
-                      "each its own host generator on a disjoint offset slice (MT19937: own seed, "
-                      "C port)" % (n_per_call, threads)}
+                      "each its own host generator on a disjoint offset slice (MT19937, MTGP32: own "
+                      "seed; MT19937 from the C port)" % (n_per_call, threads)}
 
 
 def run_reference(args):

@@ -6,7 +6,7 @@ no data collective.  Here two ranks do exactly that with the oracle (the referen
 semantics), gather their slices, and rank 0 checks that the concatenation equals one
 generator producing 2n outputs -- counter engines (Philox, ThreeFry) with one- and two-word
 distributions, stateful engines (XORWOW, MRG32k3a, LFSR113) with one-word ones.  Where no
-offset selects the slice (MT19937; a stateful engine consuming two values per output, whose
+offset selects the slice (MT19937, MTGP32; a stateful engine consuming two values per output, whose
 offsets rotate engines by values, not outputs -- checked here too) the ranks use distinct
 seeds, and the test checks their streams differ.
 """
@@ -25,7 +25,7 @@ from oracle import pyorc
 
 CASES = [(404, "uniform"), (404, "uniform_double"), (410, "uint"), (410, "normal"),
          (401, "uniform"), (402, "uniform"), (406, "uint")]
-SEEDED = [(407, "uint"), (401, "uniform_double"), (402, "normal")]
+SEEDED = [(407, "uint"), (403, "uniform"), (401, "uniform_double"), (402, "normal")]
 N = 3 * 131072 + 1000  # crosses the stateful engines' slot boundary
 
 
