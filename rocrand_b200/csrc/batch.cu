@@ -53,8 +53,8 @@ struct BatchLaunch
     uint32_t            nreq;
     unsigned long long  tiles;
     unsigned long long* next;
-    const uint32_t*     xorwow_tables;
-    const uint32_t*     xorwow_lanes;
+    const uint32_t*     xorwow_polys; // jump polynomials of the E engines
+    const uint32_t*     xorwow_seqs;  // 2 x kXorwowSeqWords words per fresh XORWOW request
     const uint64_t*     mrg_tables;
 };
 
@@ -142,10 +142,11 @@ __device__ __forceinline__ void philox_tile(const BatchReq& r, unsigned long lon
 }
 
 // Engine e of a fresh generator: the base state of its side of `start`, jumped e
-// subsequences (as the plain generator's init kernels do).  XORWOW seeds warp-cooperatively:
-// every lane of the warp must call this together.
+// subsequences (as the plain generator's init kernels do); XORWOW from the window tables of
+// the two bases, built by the block at the start of the tile.
 template<class E>
-__device__ __forceinline__ void seed_engine(const BatchReq& r, uint32_t e, E& eng, const BatchLaunch& L)
+__device__ __forceinline__ void seed_engine(const BatchReq& r, uint32_t e, E& eng, const BatchLaunch& L,
+                                            const XorwowJumpTable* tables)
 {
     const int which = e < r.start ? 1 : 0;
 #pragma unroll
@@ -153,8 +154,7 @@ __device__ __forceinline__ void seed_engine(const BatchReq& r, uint32_t e, E& en
         eng.w[k] = r.base[which][k];
     if constexpr(std::is_same_v<E, XorwowEngine>)
     {
-        const bool shared = which == __shfl_sync(0xffffffffu, which, 0);
-        xorwow_seed(eng.w, e, L.xorwow_tables, L.xorwow_lanes, shared);
+        xorwow_jump(tables[which], L.xorwow_polys, e, eng.w);
     }
     else
     {
@@ -172,7 +172,7 @@ __device__ __forceinline__ void seed_engine(const BatchReq& r, uint32_t e, E& en
 
 template<class E, class F>
 __device__ __forceinline__ void stateful_tile(const BatchReq& r, unsigned long long local, const F& f,
-                                              const BatchLaunch& L)
+                                              const BatchLaunch& L, XorwowJumpTable* tables)
 {
     using T               = typename F::T;
     constexpr unsigned VB = F::ow * sizeof(T);
@@ -181,8 +181,19 @@ __device__ __forceinline__ void stateful_tile(const BatchReq& r, unsigned long l
     const unsigned long long need = r.vec_n >= kBatchE ? kBatchE : r.vec_n + (has_edge ? 1 : 0);
     const unsigned long long t0   = local * r.units;
     const unsigned long long t1   = t0 + r.units < need ? t0 + r.units : need;
-    // the whole block steps together (seeding is warp-cooperative); lanes past t1 or without
-    // a vector of this call seed and then skip
+    if constexpr(std::is_same_v<E, XorwowEngine>)
+    {
+        if(r.arena == nullptr)
+        {
+            // slots t with t + start < E drive engines >= start (base 0), the rest base 1
+            const uint32_t* seq = L.xorwow_seqs + static_cast<size_t>(r.xseq) * 2 * kXorwowSeqWords;
+            if(t0 + r.start < kBatchE)
+                xorwow_build_jump_table(tables[0], seq, threadIdx.x, blockDim.x);
+            if(t1 - 1 + r.start >= kBatchE)
+                xorwow_build_jump_table(tables[1], seq + kXorwowSeqWords, threadIdx.x, blockDim.x);
+            __syncthreads();
+        }
+    }
     for(unsigned long long tb = t0; tb < t1; tb += blockDim.x)
     {
         const unsigned long long t     = tb + threadIdx.x;
@@ -200,9 +211,9 @@ __device__ __forceinline__ void stateful_tile(const BatchReq& r, unsigned long l
         }
         else
         {
-            seed_engine(r, e, eng, L);
             if(!loops && !edges)
                 continue;
+            seed_engine(r, e, eng, L, tables);
         }
         uint32_t           in[F::iw];
         T                  out[F::ow];
@@ -311,6 +322,7 @@ __global__ void __launch_bounds__(kBatchBlock) batch_fill(BatchLaunch L)
 {
     __shared__ unsigned long long s_tile;
     __shared__ uint32_t           s_req;
+    __shared__ XorwowJumpTable    s_xorwow[2]; // fresh XORWOW tiles: window tables of the bases
     for(;;)
     {
         if(threadIdx.x == 0)
@@ -344,10 +356,10 @@ __global__ void __launch_bounds__(kBatchBlock) batch_fill(BatchLaunch L)
                 with_plain_functor(r, [&](auto f) { philox_tile(r, local, f); });
                 break;
             case BK_XORWOW:
-                with_plain_functor(r, [&](auto f) { stateful_tile<XorwowEngine>(r, local, f, L); });
+                with_plain_functor(r, [&](auto f) { stateful_tile<XorwowEngine>(r, local, f, L, s_xorwow); });
                 break;
             case BK_MRG32K3A:
-                with_mrg_functor(r, [&](auto f) { stateful_tile<Mrg32k3aEngine>(r, local, f, L); });
+                with_mrg_functor(r, [&](auto f) { stateful_tile<Mrg32k3aEngine>(r, local, f, L, s_xorwow); });
                 break;
             default:
                 switch(r.dist)
@@ -506,12 +518,14 @@ BatchPlan::~BatchPlan()
     if(m_exec)
         cudaGraphExecDestroy(m_exec);
     cudaFree(d_reqs);
+    cudaFree(d_seq);
 }
 
 rocrand_status BatchPlan::build(const void* requests, size_t count, cudaStream_t stream)
 {
     const auto* q = static_cast<const rocrand_b200_request*>(requests);
     m_reqs.clear();
+    m_seq.clear();
     m_reqs.reserve(count);
     for(size_t i = 0; i < count; i++)
     {
@@ -541,6 +555,14 @@ rocrand_status BatchPlan::build(const void* requests, size_t count, cudaStream_t
                 memcpy(r.base, b.base, sizeof(r.base));
                 r.start = b.start;
                 r.arena = nullptr;
+                if(xw)
+                {
+                    r.xseq = static_cast<uint32_t>(m_seq.size() / (2 * kXorwowSeqWords));
+                    m_seq.resize(m_seq.size() + 2 * kXorwowSeqWords);
+                    uint32_t* seq = m_seq.data() + m_seq.size() - 2 * kXorwowSeqWords;
+                    xorwow_word_sequence(r.base[0], seq);
+                    xorwow_word_sequence(r.base[1], seq + kXorwowSeqWords);
+                }
                 break;
             }
             case ROCRAND_RNG_QUASI_DEFAULT:
@@ -603,6 +625,28 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
             m_exec = nullptr;
         }
     }
+    if(m_seq.size() > m_seq_cap)
+    {
+        cudaFree(d_seq);
+        d_seq = nullptr;
+        if(cudaMalloc(&d_seq, sizeof(uint32_t) * m_seq.size()) != cudaSuccess)
+        {
+            d_seq     = nullptr;
+            m_seq_cap = 0;
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        }
+        m_seq_cap = m_seq.size();
+        if(m_exec)
+        {
+            cudaGraphExecDestroy(m_exec);
+            m_exec = nullptr;
+        }
+    }
+    if(!m_seq.empty()
+       && cudaMemcpyAsync(d_seq, m_seq.data(), sizeof(uint32_t) * m_seq.size(), cudaMemcpyHostToDevice,
+                          stream)
+              != cudaSuccess)
+        return ROCRAND_STATUS_INTERNAL_ERROR;
     d_next = reinterpret_cast<unsigned long long*>(reinterpret_cast<unsigned char*>(d_reqs)
                                                    + sizeof(BatchReq) * m_cap);
     if(!m_reqs.empty()
@@ -640,10 +684,10 @@ rocrand_status BatchPlan::launch(cudaStream_t stream)
     L.nreq          = static_cast<uint32_t>(m_reqs.size());
     L.tiles         = m_tiles;
     L.next          = d_next;
-    L.xorwow_tables = static_cast<const uint32_t*>(stateful_digit_tables(StatefulFamily::XORWOW));
-    L.xorwow_lanes  = stateful_xorwow_lane_tables();
+    L.xorwow_polys  = stateful_xorwow_jump_polys();
+    L.xorwow_seqs   = d_seq;
     L.mrg_tables    = static_cast<const uint64_t*>(stateful_digit_tables(StatefulFamily::MRG32K3A));
-    if(L.xorwow_tables == nullptr || L.xorwow_lanes == nullptr || L.mrg_tables == nullptr)
+    if(L.xorwow_polys == nullptr || L.mrg_tables == nullptr)
         return ROCRAND_STATUS_ALLOCATION_FAILED;
     const unsigned long long want = m_tiles;
     unsigned                 grid = batch_grid();
@@ -661,8 +705,7 @@ rocrand_status BatchPlan::replay(cudaStream_t stream)
     {
         // tables and the grid are resolved before capture (their first use uploads/queries)
         (void)batch_grid();
-        if(stateful_digit_tables(StatefulFamily::XORWOW) == nullptr
-           || stateful_xorwow_lane_tables() == nullptr
+        if(stateful_xorwow_jump_polys() == nullptr
            || stateful_digit_tables(StatefulFamily::MRG32K3A) == nullptr)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
         cudaStream_t cap = nullptr;

@@ -66,6 +66,7 @@ struct BatchReq
     uint32_t        base[2][6]; // stateful: engines >= start / below start
     uint32_t        start;
     uint32_t*       arena;      // stateful resident state (nullptr: fresh, seeded from base)
+    uint32_t        xseq;       // fresh XORWOW: index of its two base word sequences
     uint32_t        sobol_offset;
     const uint32_t* sobol_v;    // the 32 direction vectors of dimension 0
 };
@@ -103,6 +104,9 @@ public:
 
 private:
     std::vector<BatchReq> m_reqs;
+    std::vector<uint32_t> m_seq;              // word sequences of fresh XORWOW requests
+    uint32_t*             d_seq     = nullptr;
+    size_t                m_seq_cap = 0;      // words
     unsigned long long    m_tiles   = 0;
     unsigned long long    m_bytes   = 0;
     BatchReq*             d_reqs    = nullptr;

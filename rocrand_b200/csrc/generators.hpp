@@ -76,8 +76,10 @@ struct StatefulBases
 StatefulBases stateful_bases(StatefulFamily fam, unsigned long long seed, unsigned long long offset);
 // Per-digit subsequence jump tables of a family on the current device (uploaded once).
 const void* stateful_digit_tables(StatefulFamily fam);
-// XORWOW lane tables J^r, r < 64, of the warp-cooperative seeding (uploaded once).
-const uint32_t* stateful_xorwow_lane_tables();
+// XORWOW jump polynomials of the E engines (word-major, uploaded once per device).
+const uint32_t* stateful_xorwow_jump_polys();
+// The 164-word sequence s_0..s_163 continued from a base state's words 0..4.
+void xorwow_word_sequence(const uint32_t* base, uint32_t* seq);
 
 // Generator of any type (api.cpp); nullptr for an unknown type.
 rocrand_generator_base_type* make_generator(rocrand_rng_type t);

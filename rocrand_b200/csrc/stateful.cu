@@ -16,8 +16,9 @@
 // keeps its engine in registers for the whole call and writes it back only if it advanced.
 // Initialisation is split: the host applies the common offset jump to the seeded state
 // once (two base states: offset/E and offset/E + 1), the device applies each engine's
-// subsequence jump J^e from per-digit tables (jump_tables.hpp), at most 9 matrix-vector
-// products per engine.
+// subsequence jump J^e: from per-digit tables (jump_tables.hpp), at most 9 matrix-vector
+// products per engine, for MRG32k3a, MRG31k3p and LFSR113; by jump polynomial for XORWOW
+// (stateful_engines.cuh: 40 shared-memory table reads per engine).
 #include "common.hpp"
 #include "dist.cuh"
 #include "generators.hpp"
@@ -31,6 +32,9 @@
 #include <mutex>
 #include <type_traits>
 #include <vector>
+
+extern "C" const unsigned char rb200_xorwow_jump_begin[];
+extern "C" const unsigned char rb200_xorwow_jump_end[];
 
 namespace rb200
 {
@@ -68,21 +72,45 @@ __global__ void __launch_bounds__(kBlock) init_gf2(InitArgs a, const uint32_t* _
         a.arena[static_cast<size_t>(k) * kE + e] = x[k];
 }
 
-// XORWOW engines: warp-cooperative seeding (stateful_engines.cuh:xorwow_seed).
-__global__ void __launch_bounds__(kBlock)
-    init_xorwow(InitArgs a, const uint32_t* __restrict__ tables, const uint32_t* __restrict__ lanes)
+// XORWOW engines by jump polynomial: each block builds the window tables of the base(s)
+// its engines use in shared memory, then each thread seeds kXorwowInitPerThread engines.
+constexpr uint32_t kXorwowInitPerThread = 2;
+
+struct XorwowInitArgs
 {
-    const uint32_t e     = blockIdx.x * kBlock + threadIdx.x; // kE is a multiple of the block
-    const int      which = e < a.start ? 1 : 0;
-    uint32_t       x[6];
+    InitArgs a;
+    uint32_t seq[2][kXorwowSeqWords]; // word sequences of base[0] and base[1]
+};
+
+__global__ void __launch_bounds__(kBlock)
+    init_xorwow(const __grid_constant__ XorwowInitArgs a, const uint32_t* __restrict__ polys)
+{
+    __shared__ XorwowJumpTable table[2];
+    __shared__ uint32_t        seq[2][kXorwowSeqWords];
+    constexpr uint32_t         per_block = kBlock * kXorwowInitPerThread;
+    const uint32_t             e0        = blockIdx.x * per_block; // kE is a multiple of it
+    const bool                 need1     = e0 < a.a.start;         // engines below start
+    const bool                 need0     = e0 + per_block > a.a.start;
+    for(uint32_t i = threadIdx.x; i < 2 * kXorwowSeqWords; i += kBlock)
+        seq[i / kXorwowSeqWords][i % kXorwowSeqWords] = a.seq[i / kXorwowSeqWords][i % kXorwowSeqWords];
+    __syncthreads();
+    if(need0)
+        xorwow_build_jump_table(table[0], seq[0], threadIdx.x, kBlock);
+    if(need1)
+        xorwow_build_jump_table(table[1], seq[1], threadIdx.x, kBlock);
+    __syncthreads();
 #pragma unroll
-    for(int k = 0; k < 6; k++)
-        x[k] = a.base[which][k];
-    const bool shared = which == __shfl_sync(0xffffffffu, which, 0);
-    xorwow_seed(x, e, tables, lanes, shared);
+    for(uint32_t k = 0; k < kXorwowInitPerThread; k++)
+    {
+        const uint32_t e     = e0 + k * kBlock + threadIdx.x;
+        const int      which = e < a.a.start ? 1 : 0;
+        uint32_t       x[5];
+        xorwow_jump(table[which], polys, e, x);
 #pragma unroll
-    for(int k = 0; k < 6; k++)
-        a.arena[static_cast<size_t>(k) * kE + e] = x[k];
+        for(int w = 0; w < 5; w++)
+            a.a.arena[static_cast<size_t>(w) * kE + e] = x[w];
+        a.a.arena[static_cast<size_t>(5) * kE + e] = a.a.base[which][5];
+    }
 }
 
 // MRG engines: two 3-word components modulo m1 and m2.
@@ -226,36 +254,50 @@ static const void* digit_tables(Family fam)
     return d;
 }
 
-// XORWOW lane tables: J^r, r = 0..63, laid out [input bit][word][r] (one upload per device).
-static const uint32_t* xorwow_lane_tables()
+// XORWOW jump polynomials p_e, e < E (derived at build time by make_xorwow_jump.c and
+// embedded by xorwow_data.S), one upload per device.
+static const uint32_t* xorwow_jump_polys()
 {
     static DeviceTables c;
     const int           dev = device_info().device;
     std::lock_guard<std::mutex> lock(c.mu);
     if(c.ptr[dev])
         return static_cast<const uint32_t*>(c.ptr[dev]);
-    const Gf2Matrix       j   = gf2_pow2(xorwow_step_matrix(), 67);
-    Gf2Matrix             acc = Gf2Matrix::identity(5);
-    std::vector<uint32_t> t(static_cast<size_t>(160) * 5 * kXorwowLaneJumps);
-    for(uint32_t r = 0; r < kXorwowLaneJumps; r++)
-    {
-        for(size_t i = 0; i < 160; i++)
-            for(size_t k = 0; k < 5; k++)
-                t[(i * 5 + k) * kXorwowLaneJumps + r] = acc.rows[i * 5 + k];
-        acc = acc.then(j);
-    }
+    const size_t bytes = static_cast<size_t>(rb200_xorwow_jump_end - rb200_xorwow_jump_begin);
+    if(bytes != sizeof(uint32_t) * 5 * kE)
+        return nullptr;
     void* d = nullptr;
-    if(cudaMalloc(&d, t.size() * 4) != cudaSuccess)
+    if(cudaMalloc(&d, bytes) != cudaSuccess)
         return nullptr;
-    if(cudaMemcpy(d, t.data(), t.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    if(cudaMemcpy(d, rb200_xorwow_jump_begin, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+    {
+        cudaFree(d);
         return nullptr;
+    }
     c.ptr[dev] = d;
     return static_cast<const uint32_t*>(d);
 }
 
-const uint32_t* stateful_xorwow_lane_tables()
+const uint32_t* stateful_xorwow_jump_polys()
 {
-    return xorwow_lane_tables();
+    return xorwow_jump_polys();
+}
+
+void xorwow_word_sequence(const uint32_t* base, uint32_t* seq)
+{
+    uint32_t x[5];
+    std::memcpy(x, base, sizeof(x));
+    std::memcpy(seq, x, sizeof(x));
+    for(int k = 5; k < kXorwowSeqWords; k++)
+    {
+        const uint32_t t = x[0] ^ (x[0] >> 2);
+        x[0]             = x[1];
+        x[1]             = x[2];
+        x[2]             = x[3];
+        x[3]             = x[4];
+        x[4]             = (x[4] ^ (x[4] << 4)) ^ (t ^ (t << 1));
+        seq[k]           = x[4];
+    }
 }
 
 // A^(2^k), k = 0..63, of the one-step map (host offset jumps), computed once per family.
@@ -556,25 +598,32 @@ public:
         a.start = m_start;
         a.arena = m_arena;
         bases_of(kFam, m_seed, m_seed4, m_offset, a.base);
-        const void* tables = digit_tables(kFam);
-        if(tables == nullptr)
-            return ROCRAND_STATUS_ALLOCATION_FAILED;
         const unsigned blocks = kE / kBlock;
         if constexpr(kFam == Family::XORWOW)
         {
-            const uint32_t* lanes = xorwow_lane_tables();
-            if(lanes == nullptr)
+            const uint32_t* polys = xorwow_jump_polys();
+            if(polys == nullptr)
                 return ROCRAND_STATUS_ALLOCATION_FAILED;
-            init_xorwow<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables), lanes);
+            XorwowInitArgs x{};
+            x.a = a;
+            xorwow_word_sequence(a.base[0], x.seq[0]);
+            xorwow_word_sequence(a.base[1], x.seq[1]);
+            init_xorwow<<<kE / (kBlock * kXorwowInitPerThread), kBlock, 0, m_stream>>>(x, polys);
         }
-        else if constexpr(kFam == Family::LFSR113)
-            init_gf2<4, 4><<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables));
-        else if constexpr(kFam == Family::MRG32K3A)
-            init_mrg<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint64_t*>(tables),
-                                                     4294967087ull, 4294944443ull);
         else
-            init_mrg<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint64_t*>(tables),
-                                                     2147483647ull, 2147462579ull);
+        {
+            const void* tables = digit_tables(kFam);
+            if(tables == nullptr)
+                return ROCRAND_STATUS_ALLOCATION_FAILED;
+            if constexpr(kFam == Family::LFSR113)
+                init_gf2<4, 4><<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint32_t*>(tables));
+            else if constexpr(kFam == Family::MRG32K3A)
+                init_mrg<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint64_t*>(tables),
+                                                         4294967087ull, 4294944443ull);
+            else
+                init_mrg<<<blocks, kBlock, 0, m_stream>>>(a, static_cast<const uint64_t*>(tables),
+                                                         2147483647ull, 2147462579ull);
+        }
         const rocrand_status st = launch_status();
         if(st != ROCRAND_STATUS_SUCCESS)
             return st;

@@ -156,85 +156,77 @@ __device__ __forceinline__ void mod_apply(const uint64_t* __restrict__ a, uint64
         x[r] = y[r];
 }
 
-// y = M x for one 160x160 GF(2) matrix (column-wise: column i = image of input bit i, 5
-// words at m + 5 i) and one x held identically by all 32 lanes of a warp: lane l folds the
-// columns of bits l, 32+l, ..., 128+l, then the partial results are XOR-reduced across the
-// warp.  25 loads and 25 shuffles per lane instead of 160 x 5 loads.
-__device__ __forceinline__ void gf2_apply_warp(const uint32_t* __restrict__ m, uint32_t* x)
+// XORWOW subsequence jumps by polynomial.  Engine e of a fresh generator is the base state
+// moved by e subsequences, J^e = A^(e 2^67) with A the 160-bit xorshift step; J^e = p_e(A)
+// for a polynomial p_e of degree < 160 (derived at build time, make_xorwow_jump.c), and
+// A^k s is the window (s_k .. s_k+4) of the word sequence that continues s.  So engine e's
+// words 0..4 are the XOR of the windows k over the set coefficients k of p_e: with the
+// 164-word sequence of the base, no matrix is needed.  The windows are grouped four
+// coefficients at a time: table entry (g, v) = XOR of the windows 4g + b over the set bits
+// b of v (g < 40, v < 16), built once per base in shared memory, so one jump is 40 table
+// reads, conflict-free (a warp's 16 possible entries of group g are 16 consecutive ones).
+constexpr int kXorwowSeqWords = 164;
+constexpr int kXorwowGroups   = 40;
+
+struct XorwowJumpTable
 {
-    const uint32_t l = threadIdx.x & 31u;
-    uint32_t       y[5] = {0u, 0u, 0u, 0u, 0u};
-#pragma unroll
-    for(int w = 0; w < 5; w++)
+    uint2    w01[kXorwowGroups * 16]; // words 0, 1
+    uint2    w23[kXorwowGroups * 16]; // words 2, 3
+    uint32_t w4[kXorwowGroups * 16];  // word 4
+};
+
+// Builds the table of one base from its word sequence (any memory space the block can
+// read); called by all `nthreads` threads of the block, which synchronise afterwards.
+__device__ __forceinline__ void xorwow_build_jump_table(XorwowJumpTable& t, const uint32_t* seq,
+                                                        uint32_t tid, uint32_t nthreads)
+{
+    for(uint32_t i = tid; i < kXorwowGroups * 16; i += nthreads)
     {
-        const uint32_t  mask = 0u - ((x[w] >> l) & 1u);
-        const uint32_t* col  = m + (32u * w + l) * 5u;
+        const uint32_t g = i >> 4, v = i & 15u;
+        uint32_t       y[5] = {0u, 0u, 0u, 0u, 0u};
 #pragma unroll
-        for(int k = 0; k < 5; k++)
-            y[k] ^= mask & __ldg(col + k);
-    }
+        for(int b = 0; b < 4; b++)
+        {
+            if((v >> b) & 1u)
+            {
 #pragma unroll
-    for(int k = 0; k < 5; k++)
-    {
-#pragma unroll
-        for(int o = 16; o > 0; o >>= 1)
-            y[k] ^= __shfl_xor_sync(0xffffffffu, y[k], o);
-        x[k] = y[k];
+                for(int j = 0; j < 5; j++)
+                    y[j] ^= seq[4 * g + b + j];
+            }
+        }
+        t.w01[i] = make_uint2(y[0], y[1]);
+        t.w23[i] = make_uint2(y[2], y[3]);
+        t.w4[i]  = y[4];
     }
 }
 
-// Lane tables of XORWOW seeding: J^r for r = 0..63 (J = one subsequence, 2^67 steps),
-// stored [input bit i][word k][r] so that a warp whose lanes apply different r reads
-// consecutive words.
-constexpr uint32_t kXorwowLaneJumps = 64;
-
-// The XORWOW engine e of a generator whose engines start from `x` (words 0..4 jumped, the
-// Weyl word 5 kept): x <- J^e x.  Must be called by all 32 lanes of the warp together
-// (it synchronises them).  e = 64 q + r: when the lanes share q and x (shared_base in every
-// lane), J^(64 q) is applied by the warp together (radix-4 digits 3..8) and J^r by each lane
-// from the lane table; otherwise each lane applies its own 9 digits.
-__device__ __forceinline__ void xorwow_seed(uint32_t* x, uint32_t e, const uint32_t* __restrict__ digits,
-                                            const uint32_t* __restrict__ lanes, bool shared_base)
+// x[0..4] <- J^e of the table's base; polys = the build-time table, word-major with stride
+// kStatefulEngines.  The Weyl word is left as it is (a subsequence jump keeps it).
+__device__ __forceinline__ void xorwow_jump(const XorwowJumpTable& t, const uint32_t* __restrict__ polys,
+                                            uint32_t e, uint32_t* x)
 {
-    constexpr size_t msize = 5 * 32 * 5;
-    const uint32_t   q     = e >> 6;
-    const uint32_t   q0    = __shfl_sync(0xffffffffu, q, 0);
-    if(!__all_sync(0xffffffffu, shared_base && q == q0))
-    {
-        for(int p = 0; p < 9; p++)
-        {
-            const uint32_t d = (e >> (2 * p)) & 3u;
-            if(d)
-                gf2_apply<5>(digits + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
-        }
-        return;
-    }
-    for(int p = 3; p < 9; p++)
-    {
-        const uint32_t d = (q >> (2 * (p - 3))) & 3u; // the same in every lane
-        if(d)
-            gf2_apply_warp(digits + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
-    }
-    // x is the same in every lane here, so the loop visits only its set bits, uniformly
-    const uint32_t r = e & 63u;
-    uint32_t       y[5] = {0u, 0u, 0u, 0u, 0u};
+    uint32_t c[5];
 #pragma unroll
-    for(int w = 0; w < 5; w++)
+    for(int j = 0; j < 5; j++)
+        c[j] = __ldg(polys + static_cast<size_t>(j) * kStatefulEngines + e);
+    uint32_t y0 = 0u, y1 = 0u, y2 = 0u, y3 = 0u, y4 = 0u;
+#pragma unroll
+    for(int g = 0; g < kXorwowGroups; g++)
     {
-        uint32_t bits = x[w];
-        while(bits)
-        {
-            const int       b   = __ffs(bits) - 1;
-            const uint32_t* row = lanes + static_cast<size_t>((32 * w + b) * 5) * kXorwowLaneJumps + r;
-            bits &= bits - 1;
-#pragma unroll
-            for(int k = 0; k < 5; k++)
-                y[k] ^= __ldg(row + k * kXorwowLaneJumps);
-        }
+        const uint32_t i = 16u * g + ((c[g >> 3] >> (4 * (g & 7))) & 15u);
+        const uint2    a = t.w01[i];
+        const uint2    b = t.w23[i];
+        y0 ^= a.x;
+        y1 ^= a.y;
+        y2 ^= b.x;
+        y3 ^= b.y;
+        y4 ^= t.w4[i];
     }
-#pragma unroll
-    for(int k = 0; k < 5; k++)
-        x[k] = y[k];
+    x[0] = y0;
+    x[1] = y1;
+    x[2] = y2;
+    x[3] = y3;
+    x[4] = y4;
 }
 
 template<class T, unsigned N>
