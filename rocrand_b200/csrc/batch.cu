@@ -53,6 +53,7 @@ struct BatchLaunch
     uint32_t            nreq;
     unsigned long long  tiles;
     unsigned long long* next;
+    const uint32_t*     tile_req;     // request index of every tile
     const uint32_t*     xorwow_polys; // jump polynomials of the E engines
     const uint32_t*     xorwow_seqs;  // 2 x kXorwowSeqWords words per fresh XORWOW request
     const uint64_t*     mrg_tables;
@@ -105,16 +106,33 @@ __device__ __forceinline__ void philox_tile(const BatchReq& r, unsigned long lon
     const BatchPhilox&       p  = r.philox;
     const unsigned long long v0 = local * r.units;
     const unsigned long long v1 = v0 + r.units < r.vec_n ? v0 + r.units : r.vec_n;
-    for(unsigned long long j = v0 + threadIdx.x; j < v1; j += blockDim.x)
+    if(p.fast)
     {
-        const uint32_t           adj = (j & (kPhiloxRefStride - 1)) == 0 ? p.start0 : p.head;
-        const unsigned long long q   = p.s0 + adj + 4 * j;
-        const uint4              c   = ctr_add(p.c0, q >> 2);
-        const uint32_t           s   = static_cast<uint32_t>(q & 3);
-        uint4                    b   = philox_block(c, p.keys);
-        if(s != 0)
-            b = interleave4(b, philox_block(ctr_add(c, 1), p.keys), s);
-        store16_cs(r.vec + j * 16, philox_vec(f, b));
+        // two independent vectors per iteration so that the multiply chains interleave
+        unsigned long long j = v0 + threadIdx.x;
+        for(; j + blockDim.x < v1; j += 2 * blockDim.x)
+        {
+            const uint4 b0 = philox_block_lane(p.x0 + static_cast<uint32_t>(j), p.lane, p.keys);
+            const uint4 b1 = philox_block_lane(p.x0 + static_cast<uint32_t>(j + blockDim.x), p.lane, p.keys);
+            store16_cs(r.vec + j * 16, philox_vec(f, b0));
+            store16_cs(r.vec + (j + blockDim.x) * 16, philox_vec(f, b1));
+        }
+        if(j < v1)
+            store16_cs(r.vec + j * 16, philox_vec(f, philox_block_lane(p.x0 + static_cast<uint32_t>(j), p.lane, p.keys)));
+    }
+    else
+    {
+        for(unsigned long long j = v0 + threadIdx.x; j < v1; j += blockDim.x)
+        {
+            const uint32_t           adj = (j & (kPhiloxRefStride - 1)) == 0 ? p.start0 : p.head;
+            const unsigned long long q   = p.s0 + adj + 4 * j;
+            const uint4              c   = ctr_add(p.c0, q >> 2);
+            const uint32_t           s   = static_cast<uint32_t>(q & 3);
+            uint4                    b   = philox_block(c, p.keys);
+            if(s != 0)
+                b = interleave4(b, philox_block(ctr_add(c, 1), p.keys), s);
+            store16_cs(r.vec + j * 16, philox_vec(f, b));
+        }
     }
     if(local == 0 && threadIdx.x == 0 && (p.head > 0 || p.tail > 0))
     {
@@ -318,36 +336,42 @@ __device__ __forceinline__ void sobol_tile(const BatchReq& r, unsigned long long
     }
 }
 
-__global__ void __launch_bounds__(kBatchBlock) batch_fill(BatchLaunch L)
+__global__ void __launch_bounds__(kBatchBlock, 4) batch_fill(BatchLaunch L)
 {
-    __shared__ unsigned long long s_tile;
+    // Tiles come from a global counter; thread 0 keeps the next two in flight so that their
+    // counter and request-map reads overlap the current tile's work: while tile t runs, the
+    // request of the next tile and the index of the one after it are being fetched.
+    __shared__ unsigned long long s_tile, s_next;
     __shared__ uint32_t           s_req;
     __shared__ XorwowJumpTable    s_xorwow[2]; // fresh XORWOW tiles: window tables of the bases
+    if(threadIdx.x == 0)
+    {
+        const unsigned long long t = atomicAdd(L.next, 1ull);
+        s_tile                     = t;
+        s_req                      = t < L.tiles ? L.tile_req[t] : 0u;
+        s_next                     = atomicAdd(L.next, 1ull);
+    }
+    __syncthreads();
     for(;;)
     {
-        if(threadIdx.x == 0)
-        {
-            const unsigned long long t = atomicAdd(L.next, 1ull);
-            s_tile                     = t;
-            if(t < L.tiles)
-            {
-                // the last request whose first tile is <= t
-                uint32_t lo = 0, hi = L.nreq - 1;
-                while(lo < hi)
-                {
-                    const uint32_t mid = (lo + hi + 1) / 2;
-                    if(L.reqs[mid].tile0 <= t)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                s_req = lo;
-            }
-        }
-        __syncthreads();
         const unsigned long long t = s_tile;
         if(t >= L.tiles)
             return;
+        unsigned long long next = 0, after = 0;
+        uint32_t           next_req = 0;
+        if(threadIdx.x == 0)
+        {
+            next = s_next;
+            if(next < L.tiles)
+            {
+                next_req = L.tile_req[next];
+                after    = atomicAdd(L.next, 1ull);
+            }
+            else
+            {
+                after = next;
+            }
+        }
         const BatchReq&          r     = L.reqs[s_req];
         const unsigned long long local = t - r.tile0;
         switch(r.kind)
@@ -378,6 +402,13 @@ __global__ void __launch_bounds__(kBatchBlock) batch_fill(BatchLaunch L)
                 break;
         }
         __syncthreads();
+        if(threadIdx.x == 0)
+        {
+            s_tile = next;
+            s_req  = next_req;
+            s_next = after;
+        }
+        __syncthreads();
     }
 }
 
@@ -390,7 +421,7 @@ BatchTuning& batch_tuning()
         BatchTuning d{};
         for(uint32_t k = 0; k < BK_COUNT; k++)
             for(uint32_t dd = 0; dd < BD_COUNT; dd++)
-                d.units[k][dd] = k == BK_PHILOX ? 2048u : (k == BK_SOBOL32 ? 8192u : 256u);
+                d.units[k][dd] = k == BK_PHILOX ? 4096u : (k == BK_SOBOL32 ? 8192u : (k == BK_XORWOW ? 1024u : 256u));
         d.blocks_per_sm = 0; // 0: occupancy
         return d;
     }();
@@ -478,6 +509,17 @@ rocrand_status batch_layout(BatchReq& r, void* output, size_t n)
         r.vec              = r.data + mis * tsize;
         r.head             = r.philox.head;
         r.tail             = r.philox.tail;
+        r.philox.fast      = 0;
+        if(r.philox.start0 == r.philox.head && ((r.philox.s0 + r.philox.head) & 3u) == 0)
+        {
+            const uint4 cbase = ctr_add(r.philox.c0, (r.philox.s0 + r.philox.head) >> 2);
+            if(static_cast<unsigned long long>(cbase.x) + r.vec_n <= (1ull << 32))
+            {
+                r.philox.fast = 1;
+                r.philox.x0   = cbase.x;
+                r.philox.lane = philox_lane(cbase, r.philox.keys);
+            }
+        }
     }
     else if(r.kind == BK_SOBOL32)
     {
@@ -519,6 +561,7 @@ BatchPlan::~BatchPlan()
         cudaGraphExecDestroy(m_exec);
     cudaFree(d_reqs);
     cudaFree(d_seq);
+    cudaFree(d_tile_req);
 }
 
 rocrand_status BatchPlan::build(const void* requests, size_t count, cudaStream_t stream)
@@ -596,12 +639,15 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
     const BatchTuning& tune = batch_tuning();
     m_tiles                 = 0;
     m_bytes                 = 0;
-    for(auto& r : m_reqs)
+    m_tile_req.clear();
+    for(size_t i = 0; i < m_reqs.size(); i++)
     {
-        r.units = tune.units[r.kind][r.dist];
-        r.tile0 = m_tiles;
+        BatchReq& r = m_reqs[i];
+        r.units     = tune.units[r.kind][r.dist];
+        r.tile0     = m_tiles;
         m_tiles += tiles_of(r);
         m_bytes += r.n * batch_elem_size(r.dist);
+        m_tile_req.resize(m_tiles, static_cast<uint32_t>(i));
     }
     int dev = 0;
     if(cudaGetDevice(&dev) != cudaSuccess)
@@ -642,6 +688,28 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
             m_exec = nullptr;
         }
     }
+    if(m_tile_req.size() > m_tile_cap)
+    {
+        cudaFree(d_tile_req);
+        d_tile_req = nullptr;
+        if(cudaMalloc(&d_tile_req, sizeof(uint32_t) * m_tile_req.size()) != cudaSuccess)
+        {
+            d_tile_req = nullptr;
+            m_tile_cap = 0;
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        }
+        m_tile_cap = m_tile_req.size();
+        if(m_exec)
+        {
+            cudaGraphExecDestroy(m_exec);
+            m_exec = nullptr;
+        }
+    }
+    if(!m_tile_req.empty()
+       && cudaMemcpyAsync(d_tile_req, m_tile_req.data(), sizeof(uint32_t) * m_tile_req.size(),
+                          cudaMemcpyHostToDevice, stream)
+              != cudaSuccess)
+        return ROCRAND_STATUS_INTERNAL_ERROR;
     if(!m_seq.empty()
        && cudaMemcpyAsync(d_seq, m_seq.data(), sizeof(uint32_t) * m_seq.size(), cudaMemcpyHostToDevice,
                           stream)
@@ -684,6 +752,7 @@ rocrand_status BatchPlan::launch(cudaStream_t stream)
     L.nreq          = static_cast<uint32_t>(m_reqs.size());
     L.tiles         = m_tiles;
     L.next          = d_next;
+    L.tile_req      = d_tile_req;
     L.xorwow_polys  = stateful_xorwow_jump_polys();
     L.xorwow_seqs   = d_seq;
     L.mrg_tables    = static_cast<const uint64_t*>(stateful_digit_tables(StatefulFamily::MRG32K3A));
@@ -873,7 +942,7 @@ extern "C" rocrand_status ROCRANDAPI rocrand_b200_autotune_batch(cudaStream_t st
                                                   ROCRAND_RNG_PSEUDO_MRG32K3A,
                                                   ROCRAND_RNG_QUASI_SOBOL32};
         const std::vector<uint32_t> cand[BK_COUNT]
-            = {{512, 1024, 2048, 4096, 8192}, {128, 256, 512, 1024}, {128, 256, 512, 1024},
+            = {{1024, 2048, 4096, 8192, 16384}, {256, 512, 1024, 2048, 4096}, {128, 256, 512, 1024, 2048},
                {2048, 4096, 8192, 16384, 32768}};
         BatchTuning&   tune = batch_tuning();
         rocrand_status st   = ROCRAND_STATUS_SUCCESS;

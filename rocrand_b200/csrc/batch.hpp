@@ -41,6 +41,10 @@ struct BatchPhilox
     PhiloxKeys keys;
     uint4      c0;
     uint32_t   s0, head, start0, tail;
+    // aligned requests whose counters keep their upper words (vector j = block x0 + j):
+    // rounds 1-2 of the words that do not vary precomputed, as in the plain fast kernel
+    uint32_t   fast, x0;
+    PhiloxLane lane;
 };
 
 // One request as the kernel sees it.
@@ -104,6 +108,9 @@ public:
 
 private:
     std::vector<BatchReq> m_reqs;
+    std::vector<uint32_t> m_tile_req;         // request index of every tile
+    uint32_t*             d_tile_req = nullptr;
+    size_t                m_tile_cap = 0;
     std::vector<uint32_t> m_seq;              // word sequences of fresh XORWOW requests
     uint32_t*             d_seq     = nullptr;
     size_t                m_seq_cap = 0;      // words
