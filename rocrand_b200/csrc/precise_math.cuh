@@ -90,27 +90,29 @@ RB_PM_HD void two_sum(double a, double b, double& s, double& e)
     e              = (a - (s - bb)) + (b - bb);
 }
 
+// s + e == a + b exactly when a == 0 or |a| >= |b| (Dekker's fast two-sum)
+RB_PM_HD void fast_two_sum(double a, double b, double& s, double& e)
+{
+    s = a + b;
+    e = b - (s - a);
+}
+
 // Natural logarithm, near-correctly rounded.
 RB_PM_HD double log(double x)
 {
-    if(!(x > 0.0)) // zero, negative, NaN
-        return x == 0.0 ? -INFINITY : NAN;
-    if(x == INFINITY)
-        return x;
-    int e = 0;
-    if(x < 0x1p-1022) // subnormal
-    {
-        x *= 0x1p54;
-        e = -54;
-    }
-    const uint64_t u = bits_of(x);
+    // The main path runs for every input (the special cases are selected at the end, so
+    // that independent calls can interleave): zero, negative, NaN and infinity still give
+    // a table row in range there.
+    const double   x0  = x;
+    const bool     sub = x < 0x1p-1022; // subnormal (or zero / negative: replaced below)
+    x                  = sub ? x * 0x1p54 : x;
+    int            e   = sub ? -54 : 0;
+    const uint64_t u   = bits_of(x);
     e += static_cast<int>((u >> 52) & 0x7ff) - 1023;
-    double m = from_bits((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull); // [1, 2)
-    if(m >= 1.4142135623730951)
-    {
-        m *= 0.5;
-        e += 1;
-    }
+    double     m  = from_bits((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull); // [1, 2)
+    const bool up = m >= 1.4142135623730951;
+    m             = up ? m * 0.5 : m;
+    e += up ? 1 : 0;
     const int     i   = static_cast<int>(rint((m - 1.0) * 128.0));
     const double* row = log_table() + 3 * (i - RB_LOG_TABLE_MIN);
     const double  invc = row[0], lch = row[1], lcl = row[2];
@@ -124,11 +126,9 @@ RB_PM_HD double log(double x)
     const double r2l = fma_(rh, rh, -r2h) + 2.0 * rh * rl;
     const double qh  = -0.5 * r2h;
     const double ql  = -0.5 * r2l;
-    // r^3 (1/3 - r/4 + r^2/5 - ...), |r| < 2^-7
-    double t = -1.0 / 12.0;
-    t        = fma_(t, rh, 1.0 / 11.0);
-    t        = fma_(t, rh, -1.0 / 10.0);
-    t        = fma_(t, rh, 1.0 / 9.0);
+    // r^3 (1/3 - r/4 + ... + r^6/9), |r| < 2^-7.5: the first term left out, r^10/10, is
+    // below 2^-75 of the result
+    double t = 1.0 / 9.0;
     t        = fma_(t, rh, -1.0 / 8.0);
     t        = fma_(t, rh, 1.0 / 7.0);
     t        = fma_(t, rh, -1.0 / 6.0);
@@ -138,11 +138,14 @@ RB_PM_HD double log(double x)
     const double tail = t * (rh * r2h);
     const double de   = static_cast<double>(e);
     double       s1h, s1l, s2h, s2l, s3h, s3l;
-    two_sum(de * RB_LN2_HI, lch, s1h, s1l); // e * ln2_hi is exact (42-bit head)
-    two_sum(s1h, rh, s2h, s2l);
-    two_sum(s2h, qh, s3h, s3l);
+    // Fast two-sums: |e ln2| >= 0.69 > |log c| <= 0.35 unless e = 0; |log c| >= 2^-7 > |r|
+    // unless c = 1 (then log c = 0); |r| > r^2/2.  e * ln2_hi is exact (42-bit head).
+    fast_two_sum(de * RB_LN2_HI, lch, s1h, s1l);
+    fast_two_sum(s1h, rh, s2h, s2l);
+    fast_two_sum(s2h, qh, s3h, s3l);
     const double low = (((s1l + s2l) + s3l) + (ql + rl)) + ((lcl + de * RB_LN2_LO) + tail);
-    return s3h + low;
+    const double y   = s3h + low;
+    return x0 > 0.0 ? (x0 == INFINITY ? x0 : y) : (x0 == 0.0 ? -INFINITY : NAN);
 }
 
 // sin and cos of x for 0 <= x < 8 (the Box-Muller angles 0 .. 2 pi), near-correctly rounded.
@@ -162,27 +165,21 @@ RB_PM_HD void sincos(double x, double& s_out, double& c_out)
         rh             = h;
     }
     const bool neg = rh < 0.0;
-    if(neg)
-    {
-        rh = -rh;
-        rl = -rl;
-    }
+    rh             = neg ? -rh : rh;
+    rl             = neg ? -rl : rl;
     const int     j   = static_cast<int>(rint(rh * 64.0));
     const double* row = sc_table() + 4 * j;
     const double  sh = row[0], sl = row[1], ch = row[2], cl = row[3];
     const double  bh = rh - static_cast<double>(j) * (1.0 / 64.0); // exact
     const double  bl = rl;
     const double  b2 = bh * bh;
-    // sin b - bh = bl + bh^3 (-1/6 + b^2/120 - ...);  cos b - 1 = -b^2/2 + b^4/24 - ...
-    double sp = -1.0 / 39916800.0;
-    sp        = fma_(sp, b2, 1.0 / 362880.0);
-    sp        = fma_(sp, b2, -1.0 / 5040.0);
+    // sin b - bh = bl + bh^3 (-1/6 + b^2/120 - b^4/5040);  cos b - 1 = -b^2/2 + b^4 (1/24 -
+    // b^2/720); |b| <= 2^-7, the first terms left out (b^9/9!, b^8/8!) are below 2^-71
+    double sp = -1.0 / 5040.0;
     sp        = fma_(sp, b2, 1.0 / 120.0);
     sp        = fma_(sp, b2, -1.0 / 6.0);
     const double sinb_rest = fma_(sp * b2, bh, bl); // bl + bh^3 S(b^2)
-    double       cp        = -1.0 / 3628800.0;
-    cp                     = fma_(cp, b2, 1.0 / 40320.0);
-    cp                     = fma_(cp, b2, -1.0 / 720.0);
+    double       cp        = -1.0 / 720.0;
     cp                     = fma_(cp, b2, 1.0 / 24.0);
     // cos b - 1 = -b^2/2 + b^4 C(b^2), with b^2 including the low part of b
     const double bb  = fma_(2.0 * bh, bl, b2);
@@ -191,36 +188,23 @@ RB_PM_HD void sincos(double x, double& s_out, double& c_out)
     const double psh = ch * bh;
     const double psl = fma_(ch, bh, -psh);
     double       ssh, ssl;
-    two_sum(sh, psh, ssh, ssl);
+    fast_two_sum(sh, psh, ssh, ssl); // sin a >= sin(1/64) > |cos a * b| unless a = 0
     const double s_low = ((ssl + psl) + sl) + ((sh * cm1 + ch * sinb_rest) + cl * bh);
     const double sv    = ssh + s_low;
     // cos(a + b) = cos a - (sin a * b) + cos a * (cos b - 1) - sin a * (sin b - b)
     const double pch = sh * bh;
     const double pcl = fma_(sh, bh, -pch);
     double       csh, csl;
-    two_sum(ch, -pch, csh, csl);
+    fast_two_sum(ch, -pch, csh, csl); // cos a >= 0.7 > |sin a * b|
     const double c_low = ((csl - pcl) + cl) + ((ch * cm1 - sh * sinb_rest) - sl * bh);
     const double cv    = csh + c_low;
     const double s     = neg ? -sv : sv;
-    switch(k & 3)
-    {
-        case 0:
-            s_out = s;
-            c_out = cv;
-            break;
-        case 1:
-            s_out = cv;
-            c_out = -s;
-            break;
-        case 2:
-            s_out = -s;
-            c_out = -cv;
-            break;
-        default:
-            s_out = -cv;
-            c_out = s;
-            break;
-    }
+    // quadrant k: (sin, cos) = (s, c), (c, -s), (-s, -c), (-c, s)
+    const bool   odd   = (k & 1) != 0;
+    const double so    = odd ? cv : s;
+    const double co    = odd ? s : cv;
+    s_out              = (k & 2) ? -so : so;
+    c_out              = ((k + 1) & 2) ? -co : co;
 }
 
 // Natural logarithm of a float, correctly rounded except in rare double-rounding cases.
