@@ -107,20 +107,26 @@ rocrand_status ROCRANDAPI rocrand_create_generator(rocrand_generator* generator,
     });
 }
 
+// Host generators (rocrand.cpp:118-160): outputs in host memory, values of the device
+// generator of the same type (host_generator.cpp).
 rocrand_status ROCRANDAPI rocrand_create_generator_host(rocrand_generator* generator,
                                                         rocrand_rng_type   rng_type)
 {
-    (void)generator;
-    (void)rng_type;
-    return ROCRAND_STATUS_TYPE_ERROR;
+    if(generator == nullptr)
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    return guarded([&] {
+        rocrand_generator_base_type* g = make_host_generator(rng_type);
+        if(g == nullptr)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        *generator = g;
+        return ROCRAND_STATUS_SUCCESS;
+    });
 }
 
 rocrand_status ROCRANDAPI rocrand_create_generator_host_blocking(rocrand_generator* generator,
                                                                  rocrand_rng_type   rng_type)
 {
-    (void)generator;
-    (void)rng_type;
-    return ROCRAND_STATUS_TYPE_ERROR;
+    return rocrand_create_generator_host(generator, rng_type);
 }
 
 rocrand_status ROCRANDAPI rocrand_destroy_generator(rocrand_generator generator)

@@ -83,6 +83,8 @@ void xorwow_word_sequence(const uint32_t* base, uint32_t* seq);
 
 // Generator of any type (api.cpp); nullptr for an unknown type.
 rocrand_generator_base_type* make_generator(rocrand_rng_type t);
+// A host generator: the device generator of type t writing through to host memory.
+rocrand_generator_base_type* make_host_generator(rocrand_rng_type t);
 
 // Factories of the other generator families (one translation unit each).
 rocrand_generator_base_type* make_threefry(rocrand_rng_type t);

@@ -98,6 +98,31 @@ def test_discrete_null_arguments(lib):
     assert lib.rocrand_destroy_discrete_distribution(None) == rb.ROCRAND_STATUS_OUT_OF_RANGE
 
 
+def test_host_generator_creation(lib):
+    """rocrand_create_generator_host(_blocking) (rocrand.cpp:118-160): every type is created,
+    setters keep their meaning, unknown types give TYPE_ERROR, NULL out-pointer OUT_OF_RANGE."""
+    import ctypes
+    for create in (lib.rocrand_create_generator_host, lib.rocrand_create_generator_host_blocking):
+        for t in (400, 401, 402, 403, 404, 405, 406, 407, 408, 409, 410, 411, 500, 501, 502, 504, 505):
+            g = ctypes.c_void_p()
+            assert create(ctypes.byref(g), t) == 0, t
+            try:
+                if t < 500:
+                    assert lib.rocrand_set_seed(g, 7) == 0
+                    if t in (403, 407):
+                        assert lib.rocrand_set_offset(g, 5) == rb.ROCRAND_STATUS_TYPE_ERROR
+                    else:
+                        assert lib.rocrand_set_offset(g, 5) == 0
+                else:
+                    assert lib.rocrand_set_quasi_random_generator_dimensions(g, 0) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+                    assert lib.rocrand_set_quasi_random_generator_dimensions(g, 4) == 0
+            finally:
+                assert lib.rocrand_destroy_generator(g) == 0
+        g = ctypes.c_void_p()
+        assert create(ctypes.byref(g), 123) == rb.ROCRAND_STATUS_TYPE_ERROR
+        assert create(None, 400) == rb.ROCRAND_STATUS_OUT_OF_RANGE
+
+
 def test_mtgp32_host_side_semantics(lib):
     """MTGP32 (mtgp32.hpp:389-416): no offset, the four pseudo orderings, no 64-bit output."""
     st, g = _create(lib, rb.ROCRAND_RNG_PSEUDO_MTGP32)
