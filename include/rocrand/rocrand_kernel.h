@@ -4,7 +4,8 @@
  *
  * Drop-in for the reference's device API (library/include/rocrand/rocrand_kernel.h and the
  * engine and distribution headers it includes) for these states:
- *   rocrand_state_philox4x32_10, rocrand_state_mrg32k3a, rocrand_state_mrg31k3p,
+ *   rocrand_state_philox4x32_10, rocrand_state_xorwow, rocrand_state_mrg32k3a,
+ *   rocrand_state_mrg31k3p,
  *   rocrand_state_threefry2x32_20, rocrand_state_threefry2x64_20,
  *   rocrand_state_threefry4x32_20, rocrand_state_threefry4x64_20,
  *   rocrand_state_sobol32, rocrand_state_scrambled_sobol32,
@@ -913,6 +914,103 @@ struct rocrand_state_mrg31k3p
     }
 };
 
+/* XORWOW (rocrand_xorwow.h:60-208): Marsaglia's xorshift160 plus a Weyl counter.  Skips
+ * by values and by subsequences (2^67 values) are taken base 4: each nonzero digit d at
+ * position i applies the polynomial x^(d 4^i) (or x^(d 4^i 2^67)) modulo the characteristic
+ * polynomial of the xorshift step to the state -- the same map as the reference's jump
+ * matrices, as 160 steps of a copy of the state and the XOR of the states at the set
+ * coefficients. */
+struct rocrand_state_xorwow
+{
+    unsigned int d;
+    unsigned int boxmuller_float_state;
+    unsigned int boxmuller_double_state;
+    float        boxmuller_float;
+    double       boxmuller_double;
+    unsigned int x[5];
+
+    ROCRAND_B200_FN static void step(unsigned int* v)
+    {
+        const unsigned int t = v[0] ^ (v[0] >> 2);
+        v[0]                 = v[1];
+        v[1]                 = v[2];
+        v[2]                 = v[3];
+        v[3]                 = v[4];
+        v[4]                 = (v[4] ^ (v[4] << 4)) ^ (t ^ (t << 1));
+    }
+    ROCRAND_B200_FN unsigned int next()
+    {
+        step(x);
+        d += 362437;
+        return d + x[4];
+    }
+    // x <- q(A) x for a polynomial q of degree < 160 (5 words)
+    ROCRAND_B200_FN void apply(const unsigned int* q)
+    {
+        unsigned int v[5] = {x[0], x[1], x[2], x[3], x[4]};
+        unsigned int y[5] = {0, 0, 0, 0, 0};
+        for(int w = 0; w < 5; w++)
+        {
+            const unsigned int bits = q[w];
+            for(int b = 0; b < 32; b++)
+            {
+                const unsigned int m = 0u - ((bits >> b) & 1u);
+#pragma unroll
+                for(int k = 0; k < 5; k++)
+                    y[k] ^= m & v[k];
+                step(v);
+            }
+        }
+#pragma unroll
+        for(int k = 0; k < 5; k++)
+            x[k] = y[k];
+    }
+    ROCRAND_B200_FN void jump(const unsigned int* table, unsigned long long n)
+    {
+        int i = 0;
+        while(n > 0)
+        {
+            const unsigned int dg = static_cast<unsigned int>(n & 3u);
+            if(dg)
+                apply(table + (3 * i + (dg - 1)) * 5);
+            n >>= 2;
+            i++;
+        }
+    }
+    ROCRAND_B200_FN void skip_values(unsigned long long offset)
+    {
+        jump(ROCRAND_B200_TABLE(xorwow_poly), offset);
+        d += static_cast<unsigned int>(offset) * 362437;
+    }
+    ROCRAND_B200_FN void skip_subsequences(unsigned long long subsequence)
+    {
+        jump(ROCRAND_B200_TABLE(xorwow_poly_sub), subsequence);
+    }
+    ROCRAND_B200_FN void seed(unsigned long long s, unsigned long long subsequence, unsigned long long offset)
+    {
+        x[0]                  = 123456789U;
+        x[1]                  = 362436069U;
+        x[2]                  = 521288629U;
+        x[3]                  = 88675123U;
+        x[4]                  = 5783321U;
+        d                     = 6615241U;
+        const unsigned int s0 = static_cast<unsigned int>(s) ^ 0x2c7f967fU;
+        const unsigned int s1 = static_cast<unsigned int>(s >> 32) ^ 0xa03697cbU;
+        const unsigned int t0 = 1228688033U * s0;
+        const unsigned int t1 = 2073658381U * s1;
+        x[0] += t0;
+        x[1] ^= t0;
+        x[2] += t1;
+        x[3] ^= t1;
+        x[4] += t0;
+        d += t1 + t0;
+        skip_subsequences(subsequence);
+        skip_values(offset);
+        boxmuller_float_state  = 0;
+        boxmuller_double_state = 0;
+    }
+};
+
 /* ThreeFry states (rocrand_threefry{2,4}_impl.h, rocrand_threefry{2x32,2x64,4x32,4x64}_20.h):
  * counter and key vectors of N words of type T, the current block and the position in it. */
 template<class T, class V, int N>
@@ -1095,6 +1193,11 @@ ROCRAND_B200_FN void rocrand_init(const unsigned long long seed, const unsigned 
 {
     state->seed(seed, subsequence, offset);
 }
+ROCRAND_B200_FN void rocrand_init(const unsigned long long seed, const unsigned long long subsequence,
+                                  const unsigned long long offset, rocrand_state_xorwow* state)
+{
+    state->seed(seed, subsequence, offset);
+}
 /* ThreeFry keys (rocrand_threefry{2x32,2x64,4x32,4x64}_20.h seed()): 2x32 {lo, hi};
  * 2x64 {seed, seed >> 32}; 4x32 and 4x64 {seed, seed >> 16, seed >> 32, seed >> 48}. */
 ROCRAND_B200_FN void rocrand_init(const unsigned long long seed, const unsigned long long subsequence,
@@ -1152,6 +1255,10 @@ ROCRAND_B200_FN unsigned int rocrand(rocrand_state_philox4x32_10* state)
 ROCRAND_B200_FN uint4 rocrand4(rocrand_state_philox4x32_10* state)
 {
     return state->next4();
+}
+ROCRAND_B200_FN unsigned int rocrand(rocrand_state_xorwow* state)
+{
+    return state->next();
 }
 /* MRG raw values are remapped from [1, m1] to 32 bits (rocrand_mrg32k3a.h:270-273,
  * rocrand_mrg31k3p.h:227-230). */
@@ -1227,6 +1334,19 @@ ROCRAND_B200_FN void skipahead_sequence(unsigned long long sequence, rocrand_sta
 {
     state->skip_subsequences(sequence);
     state->refresh();
+}
+ROCRAND_B200_FN void skipahead(unsigned long long offset, rocrand_state_xorwow* state)
+{
+    state->skip_values(offset);
+}
+ROCRAND_B200_FN void skipahead_subsequence(unsigned long long subsequence, rocrand_state_xorwow* state)
+{
+    state->skip_subsequences(subsequence);
+}
+/* an XORWOW sequence is one subsequence (rocrand_xorwow.h:300-305) */
+ROCRAND_B200_FN void skipahead_sequence(unsigned long long sequence, rocrand_state_xorwow* state)
+{
+    state->skip_subsequences(sequence);
 }
 ROCRAND_B200_FN void skipahead(unsigned long long offset, rocrand_state_mrg32k3a* state)
 {
@@ -1324,6 +1444,17 @@ ROCRAND_B200_FN double4 rocrand_uniform_double4(rocrand_state_philox4x32_10* sta
     const uint4 b = rocrand4(state);
     return double4{rocrand_b200_detail::to_double(a.x, a.y), rocrand_b200_detail::to_double(a.z, a.w),
                    rocrand_b200_detail::to_double(b.x, b.y), rocrand_b200_detail::to_double(b.z, b.w)};
+}
+
+ROCRAND_B200_FN float rocrand_uniform(rocrand_state_xorwow* state)
+{
+    return rocrand_b200_detail::to_float(rocrand(state));
+}
+ROCRAND_B200_FN double rocrand_uniform_double(rocrand_state_xorwow* state)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    return rocrand_b200_detail::to_double(a, b);
 }
 
 /* MRG uniforms: raw value in [1, m1] times 1/(m1 + 1) in double; float rounds that
@@ -1505,6 +1636,74 @@ ROCRAND_B200_FN double4 rocrand_log_normal_double4(rocrand_state_philox4x32_10* 
     const double2 r2 = rocrand_b200_detail::box_muller_double(rocrand4(state));
     return double4{exp(mean + (stddev * r1.x)), exp(mean + (stddev * r1.y)), exp(mean + (stddev * r2.x)),
                    exp(mean + (stddev * r2.y))};
+}
+
+// ---- XORWOW: Box-Muller on pairs (fp32) and quadruples (fp64) of values, one cached ----
+ROCRAND_B200_FN float rocrand_normal(rocrand_state_xorwow* state)
+{
+    if(rocrand_b200_detail::bm_has_float(state))
+        return rocrand_b200_detail::bm_take_float(state);
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    const float2       r = rocrand_b200_detail::box_muller(a, b);
+    rocrand_b200_detail::bm_keep_float(state, r.y);
+    return r.x;
+}
+ROCRAND_B200_FN float2 rocrand_normal2(rocrand_state_xorwow* state)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    return rocrand_b200_detail::box_muller(a, b);
+}
+ROCRAND_B200_FN uint4 rocrand_b200_xorwow_quad(rocrand_state_xorwow* state)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    const unsigned int c = rocrand(state);
+    const unsigned int d = rocrand(state);
+    return make_uint4(a, b, c, d);
+}
+ROCRAND_B200_FN double rocrand_normal_double(rocrand_state_xorwow* state)
+{
+    if(rocrand_b200_detail::bm_has_double(state))
+        return rocrand_b200_detail::bm_take_double(state);
+    const double2 r = rocrand_b200_detail::box_muller_double(rocrand_b200_xorwow_quad(state));
+    rocrand_b200_detail::bm_keep_double(state, r.y);
+    return r.x;
+}
+ROCRAND_B200_FN double2 rocrand_normal_double2(rocrand_state_xorwow* state)
+{
+    return rocrand_b200_detail::box_muller_double(rocrand_b200_xorwow_quad(state));
+}
+ROCRAND_B200_FN float rocrand_log_normal(rocrand_state_xorwow* state, float mean, float stddev)
+{
+    if(rocrand_b200_detail::bm_has_float(state))
+        return expf(mean + (stddev * rocrand_b200_detail::bm_take_float(state)));
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    const float2       r = rocrand_b200_detail::box_muller(a, b);
+    rocrand_b200_detail::bm_keep_float(state, r.y);
+    return expf(mean + (stddev * r.x));
+}
+ROCRAND_B200_FN float2 rocrand_log_normal2(rocrand_state_xorwow* state, float mean, float stddev)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    const float2       r = rocrand_b200_detail::box_muller(a, b);
+    return float2{expf(mean + (stddev * r.x)), expf(mean + (stddev * r.y))};
+}
+ROCRAND_B200_FN double rocrand_log_normal_double(rocrand_state_xorwow* state, double mean, double stddev)
+{
+    if(rocrand_b200_detail::bm_has_double(state))
+        return exp(mean + (stddev * rocrand_b200_detail::bm_take_double(state)));
+    const double2 r = rocrand_b200_detail::box_muller_double(rocrand_b200_xorwow_quad(state));
+    rocrand_b200_detail::bm_keep_double(state, r.y);
+    return exp(mean + (stddev * r.x));
+}
+ROCRAND_B200_FN double2 rocrand_log_normal_double2(rocrand_state_xorwow* state, double mean, double stddev)
+{
+    const double2 r = rocrand_b200_detail::box_muller_double(rocrand_b200_xorwow_quad(state));
+    return double2{exp(mean + (stddev * r.x)), exp(mean + (stddev * r.y))};
 }
 
 // ---- MRG: Box-Muller on the engine's own uniforms, one cached ----
@@ -1742,6 +1941,10 @@ ROCRAND_B200_FN uint4 rocrand_poisson4(rocrand_state_philox4x32_10* state, doubl
     const unsigned int d = rocrand_b200_detail::poisson_rejection(state, lambda);
     return uint4{a, b, c, d};
 }
+ROCRAND_B200_FN unsigned int rocrand_poisson(rocrand_state_xorwow* state, double lambda)
+{
+    return rocrand_b200_detail::poisson_rejection(state, lambda);
+}
 ROCRAND_B200_FN unsigned int rocrand_poisson(rocrand_state_mrg32k3a* state, double lambda)
 {
     return rocrand_b200_detail::poisson_rejection(state, lambda);
@@ -1785,6 +1988,11 @@ ROCRAND_B200_FN uint4 rocrand_discrete4(rocrand_state_philox4x32_10*        stat
                  rocrand_b200_detail::alias_pick(v.y, *discrete_distribution),
                  rocrand_b200_detail::alias_pick(v.z, *discrete_distribution),
                  rocrand_b200_detail::alias_pick(v.w, *discrete_distribution)};
+}
+ROCRAND_B200_FN unsigned int rocrand_discrete(rocrand_state_xorwow*               state,
+                                              const rocrand_discrete_distribution discrete_distribution)
+{
+    return rocrand_b200_detail::alias_pick(rocrand(state), *discrete_distribution);
 }
 ROCRAND_B200_FN unsigned int rocrand_discrete(rocrand_state_mrg32k3a*             state,
                                               const rocrand_discrete_distribution discrete_distribution)

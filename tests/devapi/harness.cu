@@ -301,6 +301,7 @@ extern "C" int devapi_run(int engine, int func, unsigned long long seed, int thr
         case 10:
             run_quasi<rocrand_state_scrambled_sobol64, unsigned long long><<<grid, block>>>(a, flag, true);
             break;
+        case 11: run_pseudo<rocrand_state_xorwow><<<grid, block>>>(a, flag); break;
         default: cudaFree(flag); return 2;
     }
     int unsupported = 0;

@@ -30,7 +30,7 @@ REF = os.path.join(ROOT, "oracle", "_ref", "libdevapi_ref.so")
 
 ENGINES = {"philox": 0, "mrg32k3a": 1, "mrg31k3p": 2, "threefry2x32": 3, "threefry2x64": 4,
            "threefry4x32": 5, "threefry4x64": 6, "sobol32": 7, "scrambled_sobol32": 8, "sobol64": 9,
-           "scrambled_sobol64": 10}
+           "scrambled_sobol64": 10, "xorwow": 11}
 FUNCS = {"rocrand": 0, "rocrand_block": 1, "uniform": 2, "uniform2": 3, "uniform4": 4, "uniform_double": 5,
          "uniform_double2": 6, "uniform_double4": 7, "normal": 8, "normal2": 9, "normal4": 10,
          "normal_double": 11, "normal_double2": 12, "normal_double4": 13, "log_normal": 14,
