@@ -5,7 +5,7 @@
  * Drop-in for the reference's device API (library/include/rocrand/rocrand_kernel.h and the
  * engine and distribution headers it includes) for these states:
  *   rocrand_state_philox4x32_10, rocrand_state_xorwow, rocrand_state_mrg32k3a,
- *   rocrand_state_mrg31k3p,
+ *   rocrand_state_mrg31k3p, rocrand_state_lfsr113,
  *   rocrand_state_threefry2x32_20, rocrand_state_threefry2x64_20,
  *   rocrand_state_threefry4x32_20, rocrand_state_threefry4x64_20,
  *   rocrand_state_sobol32, rocrand_state_scrambled_sobol32,
@@ -324,19 +324,24 @@ ROCRAND_B200_FN unsigned int poisson_rejection(S state, double lambda)
         return poisson_huge(state, lambda);
 }
 
+// Inversion with the cumulative sum rescaled every 500 units of lambda (Kemp's ITR).  The
+// reference computes the segment bound once (rocrand_poisson.h:138-168), so for 500 < lambda
+// < 1000 it scales by e^-1000 instead of e^-lambda and its search runs until k wraps around
+// 2^32; here the bound moves with the segment.  Results are the reference's for lambda <= 500
+// (one segment) and the correct inversion above.
 template<class S>
 ROCRAND_B200_FN unsigned int poisson_itr(S state, double lambda)
 {
     double       L;
-    double       x    = 1.0;
-    double       y    = 1.0;
-    unsigned int k    = 0;
-    int          pw   = 0;
-    double       u    = rocrand_uniform_double(state) - ROCRAND_2POW32_INV_DOUBLE / 2.0;
-    double       upow = pw + 500.0;
-    double       ex   = exp(-500.0);
+    double       x  = 1.0;
+    double       y  = 1.0;
+    unsigned int k  = 0;
+    int          pw = 0;
+    double       u  = rocrand_uniform_double(state) - ROCRAND_2POW32_INV_DOUBLE / 2.0;
+    double       ex = exp(-500.0);
     do
     {
+        const double upow = pw + 500.0;
         if(lambda > upow)
             L = ex;
         else
@@ -1011,6 +1016,81 @@ struct rocrand_state_xorwow
     }
 };
 
+/* LFSR113 (rocrand_lfsr113.h:40-160): L'Ecuyer's four Tausworthe components.  Skips by
+ * values and by subsequences (2^55 values) are taken base 4; each nonzero digit moves every
+ * component by its own polynomial: one step (the step ignores the masked low bits of a word,
+ * so its image is where the component's minimal polynomial holds), then the XOR of the
+ * component's next states at the set coefficients of x^(d 4^i S - 1) mod that polynomial --
+ * the same map as the reference's 128x128 jump matrices. */
+struct rocrand_state_lfsr113
+{
+    uint4 z;
+    uint4 subsequence; // the seed, kept as the reference's state keeps it
+
+    ROCRAND_B200_FN static unsigned int step_c(int j, unsigned int v)
+    {
+        unsigned int b;
+        switch(j)
+        {
+            case 0: b = ((v << 6) ^ v) >> 13; return ((v & 4294967294U) << 18) ^ b;
+            case 1: b = ((v << 2) ^ v) >> 27; return ((v & 4294967288U) << 2) ^ b;
+            case 2: b = ((v << 13) ^ v) >> 21; return ((v & 4294967280U) << 7) ^ b;
+            default: b = ((v << 3) ^ v) >> 12; return ((v & 4294967168U) << 13) ^ b;
+        }
+    }
+    ROCRAND_B200_FN unsigned int next()
+    {
+        unsigned int b;
+        b   = (((z.x << 6) ^ z.x) >> 13);
+        z.x = (((z.x & 4294967294U) << 18) ^ b);
+        b   = (((z.y << 2) ^ z.y) >> 27);
+        z.y = (((z.y & 4294967288U) << 2) ^ b);
+        b   = (((z.z << 13) ^ z.z) >> 21);
+        z.z = (((z.z & 4294967280U) << 7) ^ b);
+        b   = (((z.w << 3) ^ z.w) >> 12);
+        z.w = (((z.w & 4294967168U) << 13) ^ b);
+        return (z.x ^ z.y ^ z.z ^ z.w);
+    }
+    ROCRAND_B200_FN static unsigned int apply_c(int j, unsigned int q, unsigned int deg, unsigned int v)
+    {
+        unsigned int y = step_c(j, v), acc = 0;
+        for(unsigned int k = 0; k < deg; k++)
+        {
+            acc ^= (0u - ((q >> k) & 1u)) & y;
+            y = step_c(j, y);
+        }
+        return acc;
+    }
+    ROCRAND_B200_FN void jump(const unsigned int* table, unsigned long long n)
+    {
+        const unsigned int* deg = ROCRAND_B200_TABLE(lfsr113_degree);
+        int                 i   = 0;
+        while(n > 0)
+        {
+            const unsigned int dg = static_cast<unsigned int>(n & 3u);
+            if(dg)
+            {
+                const unsigned int* q = table + (3 * i + (dg - 1)) * 4;
+                z.x                   = apply_c(0, q[0], deg[0], z.x);
+                z.y                   = apply_c(1, q[1], deg[1], z.y);
+                z.z                   = apply_c(2, q[2], deg[2], z.z);
+                z.w                   = apply_c(3, q[3], deg[3], z.w);
+            }
+            n >>= 2;
+            i++;
+        }
+    }
+    ROCRAND_B200_FN void skip_values(unsigned long long n) { jump(ROCRAND_B200_TABLE(lfsr113_poly), n); }
+    ROCRAND_B200_FN void skip_subsequences(unsigned int n) { jump(ROCRAND_B200_TABLE(lfsr113_poly_sub), n); }
+    ROCRAND_B200_FN void seed(uint4 s, unsigned int sub, unsigned long long offset)
+    {
+        subsequence = s;
+        z           = s;
+        skip_subsequences(sub);
+        skip_values(offset);
+    }
+};
+
 /* ThreeFry states (rocrand_threefry{2,4}_impl.h, rocrand_threefry{2x32,2x64,4x32,4x64}_20.h):
  * counter and key vectors of N words of type T, the current block and the position in it. */
 template<class T, class V, int N>
@@ -1198,6 +1278,16 @@ ROCRAND_B200_FN void rocrand_init(const unsigned long long seed, const unsigned 
 {
     state->seed(seed, subsequence, offset);
 }
+/* LFSR113 takes its four seed words as they are (rocrand_lfsr113.h:167-180) */
+ROCRAND_B200_FN void rocrand_init(const uint4 seed, const unsigned int subsequence, rocrand_state_lfsr113* state)
+{
+    state->seed(seed, subsequence, 0);
+}
+ROCRAND_B200_FN void rocrand_init(const uint4 seed, const unsigned int subsequence, const unsigned long long offset,
+                                  rocrand_state_lfsr113* state)
+{
+    state->seed(seed, subsequence, offset);
+}
 /* ThreeFry keys (rocrand_threefry{2x32,2x64,4x32,4x64}_20.h seed()): 2x32 {lo, hi};
  * 2x64 {seed, seed >> 32}; 4x32 and 4x64 {seed, seed >> 16, seed >> 32, seed >> 48}. */
 ROCRAND_B200_FN void rocrand_init(const unsigned long long seed, const unsigned long long subsequence,
@@ -1257,6 +1347,10 @@ ROCRAND_B200_FN uint4 rocrand4(rocrand_state_philox4x32_10* state)
     return state->next4();
 }
 ROCRAND_B200_FN unsigned int rocrand(rocrand_state_xorwow* state)
+{
+    return state->next();
+}
+ROCRAND_B200_FN unsigned int rocrand(rocrand_state_lfsr113* state)
 {
     return state->next();
 }
@@ -1345,6 +1439,18 @@ ROCRAND_B200_FN void skipahead_subsequence(unsigned long long subsequence, rocra
 }
 /* an XORWOW sequence is one subsequence (rocrand_xorwow.h:300-305) */
 ROCRAND_B200_FN void skipahead_sequence(unsigned long long sequence, rocrand_state_xorwow* state)
+{
+    state->skip_subsequences(sequence);
+}
+ROCRAND_B200_FN void skipahead(unsigned long long offset, rocrand_state_lfsr113* state)
+{
+    state->skip_values(offset);
+}
+ROCRAND_B200_FN void skipahead_subsequence(unsigned int subsequence, rocrand_state_lfsr113* state)
+{
+    state->skip_subsequences(subsequence);
+}
+ROCRAND_B200_FN void skipahead_sequence(unsigned int sequence, rocrand_state_lfsr113* state)
 {
     state->skip_subsequences(sequence);
 }
@@ -1455,6 +1561,15 @@ ROCRAND_B200_FN double rocrand_uniform_double(rocrand_state_xorwow* state)
     const unsigned int a = rocrand(state);
     const unsigned int b = rocrand(state);
     return rocrand_b200_detail::to_double(a, b);
+}
+
+ROCRAND_B200_FN float rocrand_uniform(rocrand_state_lfsr113* state)
+{
+    return rocrand_b200_detail::to_float(rocrand(state));
+}
+ROCRAND_B200_FN double rocrand_uniform_double(rocrand_state_lfsr113* state)
+{
+    return rocrand_b200_detail::to_double(rocrand(state));
 }
 
 /* MRG uniforms: raw value in [1, m1] times 1/(m1 + 1) in double; float rounds that
@@ -1706,6 +1821,54 @@ ROCRAND_B200_FN double2 rocrand_log_normal_double2(rocrand_state_xorwow* state, 
     return double2{exp(mean + (stddev * r.x)), exp(mean + (stddev * r.y))};
 }
 
+// ---- LFSR113: the inverse-erf normal for single values, Box-Muller for pairs, no cache ----
+ROCRAND_B200_FN float rocrand_normal(rocrand_state_lfsr113* state)
+{
+    return rocrand_b200_detail::normal_inv(rocrand(state));
+}
+ROCRAND_B200_FN float2 rocrand_normal2(rocrand_state_lfsr113* state)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    return rocrand_b200_detail::box_muller(a, b);
+}
+ROCRAND_B200_FN double rocrand_normal_double(rocrand_state_lfsr113* state)
+{
+    return rocrand_b200_detail::normal_inv_double(rocrand(state));
+}
+ROCRAND_B200_FN uint4 rocrand_b200_lfsr113_quad(rocrand_state_lfsr113* state)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    const unsigned int c = rocrand(state);
+    const unsigned int d = rocrand(state);
+    return make_uint4(a, b, c, d);
+}
+ROCRAND_B200_FN double2 rocrand_normal_double2(rocrand_state_lfsr113* state)
+{
+    return rocrand_b200_detail::box_muller_double(rocrand_b200_lfsr113_quad(state));
+}
+ROCRAND_B200_FN float rocrand_log_normal(rocrand_state_lfsr113* state, float mean, float stddev)
+{
+    float r = rocrand_b200_detail::normal_inv(rocrand(state));
+    return expf(mean + (stddev * r));
+}
+ROCRAND_B200_FN float2 rocrand_log_normal2(rocrand_state_lfsr113* state, float mean, float stddev)
+{
+    const float2 r = rocrand_normal2(state);
+    return float2{expf(mean + (stddev * r.x)), expf(mean + (stddev * r.y))};
+}
+ROCRAND_B200_FN double rocrand_log_normal_double(rocrand_state_lfsr113* state, double mean, double stddev)
+{
+    double r = rocrand_b200_detail::normal_inv_double(rocrand(state));
+    return exp(mean + (stddev * r));
+}
+ROCRAND_B200_FN double2 rocrand_log_normal_double2(rocrand_state_lfsr113* state, double mean, double stddev)
+{
+    const double2 r = rocrand_b200_detail::box_muller_double(rocrand_b200_lfsr113_quad(state));
+    return double2{exp(mean + (stddev * r.x)), exp(mean + (stddev * r.y))};
+}
+
 // ---- MRG: Box-Muller on the engine's own uniforms, one cached ----
 #define ROCRAND_B200_MRG_NORMAL(S, NORM)                                                                   \
     ROCRAND_B200_FN float rocrand_normal(S* state)                                                         \
@@ -1945,6 +2108,10 @@ ROCRAND_B200_FN unsigned int rocrand_poisson(rocrand_state_xorwow* state, double
 {
     return rocrand_b200_detail::poisson_rejection(state, lambda);
 }
+ROCRAND_B200_FN unsigned int rocrand_poisson(rocrand_state_lfsr113* state, double lambda)
+{
+    return rocrand_b200_detail::poisson_inversion(state, lambda);
+}
 ROCRAND_B200_FN unsigned int rocrand_poisson(rocrand_state_mrg32k3a* state, double lambda)
 {
     return rocrand_b200_detail::poisson_rejection(state, lambda);
@@ -1990,6 +2157,11 @@ ROCRAND_B200_FN uint4 rocrand_discrete4(rocrand_state_philox4x32_10*        stat
                  rocrand_b200_detail::alias_pick(v.w, *discrete_distribution)};
 }
 ROCRAND_B200_FN unsigned int rocrand_discrete(rocrand_state_xorwow*               state,
+                                              const rocrand_discrete_distribution discrete_distribution)
+{
+    return rocrand_b200_detail::alias_pick(rocrand(state), *discrete_distribution);
+}
+ROCRAND_B200_FN unsigned int rocrand_discrete(rocrand_state_lfsr113*              state,
                                               const rocrand_discrete_distribution discrete_distribution)
 {
     return rocrand_b200_detail::alias_pick(rocrand(state), *discrete_distribution);

@@ -421,7 +421,11 @@ BatchTuning& batch_tuning()
         BatchTuning d{};
         for(uint32_t k = 0; k < BK_COUNT; k++)
             for(uint32_t dd = 0; dd < BD_COUNT; dd++)
+            {
                 d.units[k][dd] = k == BK_PHILOX ? 4096u : (k == BK_SOBOL32 ? 8192u : (k == BK_XORWOW ? 1024u : 256u));
+                // serving: smaller tiles keep small requests' latency low and balance mixes
+                d.serve_units[k][dd] = k == BK_PHILOX ? 2048u : (k == BK_SOBOL32 ? 8192u : 256u);
+            }
         d.blocks_per_sm = 0; // 0: occupancy
         return d;
     }();
@@ -643,7 +647,7 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
     for(size_t i = 0; i < m_reqs.size(); i++)
     {
         BatchReq& r = m_reqs[i];
-        r.units     = tune.units[r.kind][r.dist];
+        r.units     = m_serving ? tune.serve_units[r.kind][r.dist] : tune.units[r.kind][r.dist];
         r.tile0     = m_tiles;
         m_tiles += tiles_of(r);
         m_bytes += r.n * batch_elem_size(r.dist);

@@ -78,7 +78,8 @@ struct BatchReq
 // Tile sizes and grid of one (kind, dist) pair, chosen by the autotuner.
 struct BatchTuning
 {
-    uint32_t units[BK_COUNT][BD_COUNT];
+    uint32_t units[BK_COUNT][BD_COUNT];       // batches of fresh generators (autotuned)
+    uint32_t serve_units[BK_COUNT][BD_COUNT]; // serving batches: resident states, mixed sizes
     uint32_t blocks_per_sm;
 };
 
@@ -97,6 +98,8 @@ public:
     void add(const BatchReq& r) { m_reqs.push_back(r); }
     // Drops the descriptors, keeping the device table for reuse.
     void clear() { m_reqs.clear(); }
+    // Serving batches (resident states, latency-bound mixes) take the serving tile sizes.
+    void set_serving(bool serving) { m_serving = serving; }
     // Assigns tiles and uploads the table on `stream`.
     rocrand_status upload(cudaStream_t stream);
     // Launches the persistent kernel (resets the tile counter first).
@@ -108,6 +111,7 @@ public:
 
 private:
     std::vector<BatchReq> m_reqs;
+    bool                  m_serving = false;
     std::vector<uint32_t> m_tile_req;         // request index of every tile
     uint32_t*             d_tile_req = nullptr;
     size_t                m_tile_cap = 0;

@@ -156,6 +156,7 @@ public:
                 return ROCRAND_STATUS_INTERNAL_ERROR;
             m_streams.push_back(st);
             m_plans.emplace_back(new BatchPlan());
+            m_plans.back()->set_serving(true);
         }
         m_worker = std::thread([this] { loop(); });
         return ROCRAND_STATUS_SUCCESS;

@@ -175,6 +175,164 @@ void emit_xorwow(FILE* f, const char* name, int first)
     }
 }
 
+// ---- LFSR113 jump polynomials --------------------------------------------------------------
+// Each of the four Tausworthe components is linear on its 32-bit word, but its step ignores
+// the word's low bits (they are masked off), so on the whole word the step T is not
+// invertible; on its image V (dimension k = 31, 29, 28, 25) it is, with a primitive minimal
+// polynomial phi of degree k.  Hence T^N z = T^(N-1) (T z) = (x^(N-1) mod phi)(T) (T z) for
+// N >= 1 and any word z.  The device API stores x^(d 4^i S - 1) mod phi per component
+// (S = 1 for offsets, 2^55 for subsequences), i < 32, d = 1..3, one word each.
+
+uint32_t lfsr_step(int j, uint32_t z)
+{
+    uint32_t b;
+    switch(j)
+    {
+        case 0: b = ((z << 6) ^ z) >> 13; return ((z & 4294967294u) << 18) ^ b;
+        case 1: b = ((z << 2) ^ z) >> 27; return ((z & 4294967288u) << 2) ^ b;
+        case 2: b = ((z << 13) ^ z) >> 21; return ((z & 4294967280u) << 7) ^ b;
+        default: b = ((z << 3) ^ z) >> 12; return ((z & 4294967168u) << 13) ^ b;
+    }
+}
+
+struct SmallField
+{
+    uint64_t phi = 0; // minimal polynomial (bit k = coefficient of x^k)
+    int      deg = 0;
+    uint64_t mulmod(uint64_t a, uint64_t b) const
+    {
+        uint64_t acc = 0;
+        for(int i = 0; i < deg; i++)
+            if((a >> i) & 1u)
+                acc ^= b << i;
+        for(int d = 2 * deg - 2; d >= deg; d--)
+            if((acc >> d) & 1u)
+                acc ^= phi << (d - deg);
+        return acc;
+    }
+};
+
+bool lfsr_field(int j, SmallField& f)
+{
+    const int        n = 96;
+    uint32_t         z = lfsr_step(j, 0x9e3779b9u);
+    std::vector<int> s(n), c(n + 1, 0), b(n + 1, 0), t;
+    for(int i = 0; i < n; i++)
+    {
+        s[i] = static_cast<int>(z >> 31);
+        z    = lfsr_step(j, z);
+    }
+    c[0] = b[0] = 1;
+    int L = 0, m = 1;
+    for(int i = 0; i < n; i++)
+    {
+        int d = s[i];
+        for(int k = 1; k <= L; k++)
+            d ^= c[k] & s[i - k];
+        if(!d)
+        {
+            m++;
+            continue;
+        }
+        t = c;
+        for(int k = 0; k + m <= n; k++)
+            c[k + m] ^= b[k];
+        if(2 * L <= i)
+        {
+            L = i + 1 - L;
+            b = t;
+            m = 1;
+        }
+        else
+        {
+            m++;
+        }
+    }
+    const int want[4] = {31, 29, 28, 25};
+    if(L != want[j])
+        return false;
+    f.deg = L;
+    f.phi = 0;
+    for(int i = 0; i <= L; i++)
+        if(c[i])
+            f.phi |= 1ull << (L - i);
+    return (f.phi & 1u) != 0;
+}
+
+// T^N z by the stored polynomial q = x^(N-1) mod phi
+uint32_t lfsr_apply(int j, const SmallField& f, uint64_t q, uint32_t z)
+{
+    uint32_t y = lfsr_step(j, z), acc = 0;
+    for(int k = 0; k < f.deg; k++)
+    {
+        if((q >> k) & 1u)
+            acc ^= y;
+        y = lfsr_step(j, y);
+    }
+    return acc;
+}
+
+int emit_lfsr113(FILE* f)
+{
+    SmallField fld[4];
+    for(int j = 0; j < 4; j++)
+        if(!lfsr_field(j, fld[j]))
+            return 1;
+    const int  firsts[2] = {0, 55};
+    const char* names[2] = {"lfsr113_poly", "lfsr113_poly_sub"};
+    const Gf2Matrix a    = lfsr113_step_matrix();
+    for(int kind = 0; kind < 2; kind++)
+    {
+        // value[i][d-1][j]
+        std::vector<uint32_t> v(32 * 3 * 4);
+        for(int j = 0; j < 4; j++)
+        {
+            const SmallField& F   = fld[j];
+            const uint64_t    inv = F.phi >> 1; // x^-1 = (phi - 1) / x
+            uint64_t          dig = 2;           // x
+            for(int k = 0; k < firsts[kind]; k++)
+                dig = F.mulmod(dig, dig);        // x^(2^first)
+            for(int i = 0; i < 32; i++)
+            {
+                uint64_t p = dig;
+                for(int d = 1; d <= 3; d++)
+                {
+                    v[(i * 3 + (d - 1)) * 4 + j] = static_cast<uint32_t>(F.mulmod(p, inv));
+                    p                            = F.mulmod(p, dig);
+                }
+                dig = F.mulmod(dig, dig);
+                dig = F.mulmod(dig, dig);
+            }
+        }
+        // self-check on two digits against the 128-bit step matrix raised to the jump
+        for(int i : {0, 1, 3})
+        {
+            for(int d = 1; d <= 3; d++)
+            {
+                const unsigned long long e  = static_cast<unsigned long long>(d) << (2 * i);
+                Gf2Matrix                m  = gf2_pow(kind == 0 ? a : gf2_pow2(a, 55), e);
+                uint32_t                 z[4] = {0x12345679u, 0xfedcba98u, 0x0f0f0f0fu, 0xc0ffee11u}, w[4];
+                m.apply(z, w);
+                for(int j = 0; j < 4; j++)
+                    if(lfsr_apply(j, fld[j], v[(i * 3 + (d - 1)) * 4 + j], z[j]) != w[j])
+                        return 1;
+            }
+        }
+        for(int copy = 0; copy < 2; copy++)
+        {
+            std::fprintf(f, "%s const unsigned int %s_%s[32 * 3 * 4] = {\n",
+                         copy == 0 ? "static __device__" : "static", names[kind], copy == 0 ? "d" : "h");
+            for(int r = 0; r < 32 * 3; r++)
+                std::fprintf(f, "    %uu, %uu, %uu, %uu,\n", v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
+            std::fprintf(f, "};\n");
+        }
+    }
+    std::fprintf(f, "static __device__ const unsigned int lfsr113_degree_d[4] = {%d, %d, %d, %d};\n"
+                    "static const unsigned int lfsr113_degree_h[4] = {%d, %d, %d, %d};\n",
+                 fld[0].deg, fld[1].deg, fld[2].deg, fld[3].deg, fld[0].deg, fld[1].deg, fld[2].deg, fld[3].deg);
+    return 0;
+}
+
 } // namespace
 
 int main(int argc, char** argv)
@@ -241,6 +399,10 @@ int main(int argc, char** argv)
                     " * xorshift step, i < 32, d = 1..3, 5 words each (bit k = coefficient of x^k). */\n");
     emit_xorwow(f, "xorwow_poly", 0);
     emit_xorwow(f, "xorwow_poly_sub", 67);
+    std::fprintf(f, "/* LFSR113: per component, x^(d 4^i S - 1) modulo its minimal polynomial on the image of\n"
+                    " * its step (S = 1 or 2^55), i < 32, d = 1..3, words [i][d-1][component]. */\n");
+    if(emit_lfsr113(f) != 0)
+        return 1;
     std::fprintf(f, "\n} // namespace rocrand_b200_detail\n\n#endif\n");
     std::fclose(f);
     return 0;

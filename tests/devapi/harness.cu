@@ -244,7 +244,17 @@ __device__ bool call(S* s, int f, int c, const Args& a, unsigned char* slot)
 template<class S>
 __device__ void init_pseudo(S* s, const Args& a, unsigned t)
 {
-    rocrand_init(a.seed, t, 7ull * t, s);
+    if constexpr(std::is_same_v<S, rocrand_state_lfsr113>)
+    {
+        const uint4 seed = make_uint4(static_cast<unsigned int>(a.seed), static_cast<unsigned int>(a.seed >> 32),
+                                      static_cast<unsigned int>(a.seed) ^ 0x9e3779b9u,
+                                      static_cast<unsigned int>(a.seed >> 32) ^ 0x7f4a7c15u);
+        rocrand_init(seed, t, 7ull * t, s);
+    }
+    else
+    {
+        rocrand_init(a.seed, t, 7ull * t, s);
+    }
 }
 
 template<class S>
@@ -302,6 +312,7 @@ extern "C" int devapi_run(int engine, int func, unsigned long long seed, int thr
             run_quasi<rocrand_state_scrambled_sobol64, unsigned long long><<<grid, block>>>(a, flag, true);
             break;
         case 11: run_pseudo<rocrand_state_xorwow><<<grid, block>>>(a, flag); break;
+        case 12: run_pseudo<rocrand_state_lfsr113><<<grid, block>>>(a, flag); break;
         default: cudaFree(flag); return 2;
     }
     int unsupported = 0;

@@ -10,6 +10,10 @@ log-normals (both evaluate the same expressions with the same device intrinsics)
 (all three samplers: lambda below 64, up to 4000 and above) and discrete distributions,
 skip-ahead by values, subsequences and sequences, and a mix that crosses the cached second
 Box-Muller value.
+
+Poisson lambda between 500 and 1000 is never run through the reference: its inversion sampler
+(Sobol, ThreeFry, LFSR113) then searches until a 32-bit counter wraps (tens of seconds per
+call); this library's sampler moves the segment bound and is checked on the CPU instead.
 """
 
 import ctypes
@@ -30,7 +34,7 @@ REF = os.path.join(ROOT, "oracle", "_ref", "libdevapi_ref.so")
 
 ENGINES = {"philox": 0, "mrg32k3a": 1, "mrg31k3p": 2, "threefry2x32": 3, "threefry2x64": 4,
            "threefry4x32": 5, "threefry4x64": 6, "sobol32": 7, "scrambled_sobol32": 8, "sobol64": 9,
-           "scrambled_sobol64": 10, "xorwow": 11}
+           "scrambled_sobol64": 10, "xorwow": 11, "lfsr113": 12}
 FUNCS = {"rocrand": 0, "rocrand_block": 1, "uniform": 2, "uniform2": 3, "uniform4": 4, "uniform_double": 5,
          "uniform_double2": 6, "uniform_double4": 7, "normal": 8, "normal2": 9, "normal4": 10,
          "normal_double": 11, "normal_double2": 12, "normal_double4": 13, "log_normal": 14,
@@ -105,7 +109,7 @@ CASES = [("rocrand", 0, 0), ("rocrand_block", 0, 0), ("uniform", 0, 0), ("unifor
          ("normal2", 0, 0), ("normal4", 0, 0), ("normal_double", 0, 0), ("normal_double2", 0, 0),
          ("normal_double4", 0, 0), ("log_normal", 0.3, 0.7), ("log_normal2", 0.3, 0.7), ("log_normal4", 0.3, 0.7),
          ("log_normal_double", -0.2, 1.5), ("log_normal_double2", -0.2, 1.5), ("log_normal_double4", -0.2, 1.5),
-         ("poisson", 3.5, 0), ("poisson", 700.0, 0), ("poisson", 5000.0, 0), ("poisson", 1500.0, 0),
+         ("poisson", 3.5, 0), ("poisson", 300.0, 0), ("poisson", 2500.0, 0), ("poisson", 5000.0, 0),
          ("poisson4", 20.0, 0), ("discrete", 0, 0), ("discrete4", 0, 0), ("skipahead", 1000003, 0),
          ("skipahead_subsequence", 5, 0), ("skipahead_sequence", 3, 0), ("mix", 0.1, 0.9)]
 
