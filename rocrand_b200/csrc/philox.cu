@@ -92,8 +92,11 @@ __global__ void __launch_bounds__(kBlock)
     {
         const uint4 b0 = philox_block_lane(x0 + j, lane, a.keys);
         const uint4 b1 = philox_block_lane(x0 + j + stride, lane, a.keys);
-        store16_cs(a.vec + static_cast<size_t>(j) * 16, philox_vec(g, b0));
-        store16_cs(a.vec + static_cast<size_t>(j + stride) * 16, philox_vec(g, b1));
+        // both transforms before either store, so that their chains can interleave
+        const uint4 v0 = philox_vec(g, b0);
+        const uint4 v1 = philox_vec(g, b1);
+        store16_cs(a.vec + static_cast<size_t>(j) * 16, v0);
+        store16_cs(a.vec + static_cast<size_t>(j + stride) * 16, v1);
     }
     if(j < vec_n)
         store16_cs(a.vec + static_cast<size_t>(j) * 16, philox_vec(g, philox_block_lane(x0 + j, lane, a.keys)));

@@ -59,6 +59,16 @@ RB_PM_HD const double* sc_table()
 #endif
 }
 
+// read-only table entry (through the non-coherent cache on the device)
+RB_PM_HD double tab(const double* p)
+{
+#if defined(__CUDA_ARCH__)
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
 RB_PM_HD double fma_(double a, double b, double c)
 {
 #if defined(__CUDA_ARCH__)
@@ -115,7 +125,7 @@ RB_PM_HD double log(double x)
     e += up ? 1 : 0;
     const int     i   = static_cast<int>(rint((m - 1.0) * 128.0));
     const double* row = log_table() + 3 * (i - RB_LOG_TABLE_MIN);
-    const double  invc = row[0], lch = row[1], lcl = row[2];
+    const double  invc = tab(row), lch = tab(row + 1), lcl = tab(row + 2);
     // r = m * invc - 1 exactly, as r_hi + r_lo
     const double ph = m * invc;
     const double pl = fma_(m, invc, -ph);
@@ -169,7 +179,7 @@ RB_PM_HD void sincos(double x, double& s_out, double& c_out)
     rl             = neg ? -rl : rl;
     const int     j   = static_cast<int>(rint(rh * 64.0));
     const double* row = sc_table() + 4 * j;
-    const double  sh = row[0], sl = row[1], ch = row[2], cl = row[3];
+    const double  sh = tab(row), sl = tab(row + 1), ch = tab(row + 2), cl = tab(row + 3);
     const double  bh = rh - static_cast<double>(j) * (1.0 / 64.0); // exact
     const double  bl = rl;
     const double  b2 = bh * bh;

@@ -176,6 +176,8 @@ __global__ void __launch_bounds__(kBlock) stateful_fill(FillArgs a, F f)
     uint32_t           in[F::iw];
     T                  out[F::ow];
     unsigned long long j = t;
+    // unrolled so that the state words rotate back into place (no register moves per step)
+#pragma unroll(E::kUnroll)
     for(; j < a.vec_n; j += kE)
     {
 #pragma unroll

@@ -14,8 +14,9 @@ namespace rb200
 
 struct XorwowEngine // rocrand_xorwow.h:165-177
 {
-    static constexpr int kWords = 6; // x[0..4], d
-    static constexpr int kGf2   = 5; // words covered by the jump matrices
+    static constexpr int kWords  = 6; // x[0..4], d
+    static constexpr int kGf2    = 5; // words covered by the jump matrices
+    static constexpr int kUnroll = 5; // steps after which the state words are back in place
     uint32_t             w[kWords];
     __device__ __forceinline__ uint32_t next()
     {
@@ -32,8 +33,9 @@ struct XorwowEngine // rocrand_xorwow.h:165-177
 
 struct Lfsr113Engine // rocrand_lfsr113.h:146-160
 {
-    static constexpr int kWords = 4;
-    static constexpr int kGf2   = 4;
+    static constexpr int kWords  = 4;
+    static constexpr int kGf2    = 4;
+    static constexpr int kUnroll = 1;
     uint32_t             w[kWords];
     __device__ __forceinline__ uint32_t next()
     {
@@ -52,29 +54,34 @@ struct Lfsr113Engine // rocrand_lfsr113.h:146-160
 
 struct Mrg32k3aEngine // rocrand_mrg32k3a.h:160-190: g1[0..2], g2[0..2]
 {
-    static constexpr int      kWords = 6;
+    static constexpr int      kWords  = 6;
+    static constexpr int      kUnroll = 3;
     static constexpr uint64_t kM1 = 4294967087ull, kM2 = 4294944443ull;
     uint32_t                  w[kWords];
-    __device__ __forceinline__ static uint64_t mod_m1(uint64_t p)
+    // t < 2 m: t mod m, with the comparison and subtraction on 32-bit words (t - m < 2^32)
+    __device__ __forceinline__ static uint32_t sub_once(uint64_t t, uint32_t m)
     {
-        p = 209ull * (p >> 32) + (p & 0xffffffffull);
-        return p >= kM1 ? p - kM1 : p;
+        const uint32_t lo = static_cast<uint32_t>(t);
+        return (static_cast<uint32_t>(t >> 32) != 0u || lo >= m) ? lo - m : lo;
     }
-    __device__ __forceinline__ static uint64_t mod_m2(uint64_t p)
+    // p < 2^54: 2^32 = 209 (mod m1) folds p below 2^33 < 2 m1
+    __device__ __forceinline__ static uint32_t mod_m1(uint64_t p)
+    {
+        return sub_once(209ull * (p >> 32) + (p & 0xffffffffull), static_cast<uint32_t>(kM1));
+    }
+    // p < 2^54: two folds by 2^32 = 22853 (mod m2) bring p below 2^33 < 2 m2
+    __device__ __forceinline__ static uint32_t mod_m2(uint64_t p)
     {
         p = 22853ull * (p >> 32) + (p & 0xffffffffull);
-        p = 22853ull * (p >> 32) + (p & 0xffffffffull);
-        return p >= kM2 ? p - kM2 : p;
+        return sub_once(22853ull * (p >> 32) + (p & 0xffffffffull), static_cast<uint32_t>(kM2));
     }
     __device__ __forceinline__ uint32_t next()
     {
-        const uint32_t p1 = static_cast<uint32_t>(mod_m1(
-            1403580ull * w[1] + 810728ull * static_cast<uint32_t>(static_cast<uint32_t>(kM1) - w[0])));
+        const uint32_t p1 = mod_m1(1403580ull * w[1] + 810728ull * static_cast<uint32_t>(static_cast<uint32_t>(kM1) - w[0]));
         w[0] = w[1];
         w[1] = w[2];
         w[2] = p1;
-        const uint32_t p2 = static_cast<uint32_t>(mod_m2(
-            527612ull * w[5] + 1370589ull * static_cast<uint32_t>(static_cast<uint32_t>(kM2) - w[3])));
+        const uint32_t p2 = mod_m2(527612ull * w[5] + 1370589ull * static_cast<uint32_t>(static_cast<uint32_t>(kM2) - w[3]));
         w[3] = w[4];
         w[4] = w[5];
         w[5] = p2;
@@ -84,7 +91,8 @@ struct Mrg32k3aEngine // rocrand_mrg32k3a.h:160-190: g1[0..2], g2[0..2]
 
 struct Mrg31k3pEngine // rocrand_mrg31k3p.h:155-185: x1[0..2], x2[0..2]
 {
-    static constexpr int      kWords = 6;
+    static constexpr int      kWords  = 6;
+    static constexpr int      kUnroll = 3;
     static constexpr uint32_t kM1 = 2147483647u, kM2 = 2147462579u;
     uint32_t                  w[kWords];
     __device__ __forceinline__ uint32_t next()
