@@ -5,7 +5,7 @@
  * Drop-in for the reference's device API (library/include/rocrand/rocrand_kernel.h and the
  * engine and distribution headers it includes) for these states:
  *   rocrand_state_philox4x32_10, rocrand_state_xorwow, rocrand_state_mrg32k3a,
- *   rocrand_state_mrg31k3p, rocrand_state_lfsr113,
+ *   rocrand_state_mrg31k3p, rocrand_state_lfsr113, rocrand_state_mtgp32 (block-wide),
  *   rocrand_state_threefry2x32_20, rocrand_state_threefry2x64_20,
  *   rocrand_state_threefry4x32_20, rocrand_state_threefry4x64_20,
  *   rocrand_state_sobol32, rocrand_state_scrambled_sobol32,
@@ -33,8 +33,13 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "rocrand/rocrand.h"
 #include "rocrand/rocrand_b200_jump_tables.h"
 #include "rocrand/rocrand_discrete_types.h"
+
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
 
 #define ROCRAND_B200_FN __forceinline__ __host__ __device__
 
@@ -1090,6 +1095,215 @@ struct rocrand_state_lfsr113
         skip_values(offset);
     }
 };
+
+/* MTGP32 (rocrand_mtgp32.h): the block generators of Saito and Matsumoto's MTGP with
+ * Mersenne exponent 11213.  One state per thread block (its 1024-word ring, ring offset and
+ * parameter set), made on the host by rocrand_make_state_mtgp32 from the published
+ * parameter sets (rocrand/rocrand_mtgp32_11213.h); rocrand(state) is called by every thread
+ * of the block together and gives thread t the value t of the block's next 256 (blockDim.x)
+ * values. */
+#define MTGP_MEXP 11213
+#define MTGP_N 351
+#define MTGP_FLOOR_2P 256
+#define MTGP_CEIL_2P 512
+#define MTGP_TN MTGP_FLOOR_2P
+#define MTGP_LS (MTGP_TN * 3)
+#define MTGP_BN_MAX 512
+#define MTGP_TS 16
+#define MTGP_STATE 1024
+#define MTGP_MASK 1023
+
+struct mtgp32_params_fast_t
+{
+    int           mexp;
+    int           pos;
+    int           sh1;
+    int           sh2;
+    unsigned int  tbl[16];
+    unsigned int  tmp_tbl[16];
+    unsigned int  flt_tmp_tbl[16];
+    unsigned int  mask;
+    unsigned char poly_sha1[21];
+};
+typedef mtgp32_params_fast_t mtgp32_fast_params;
+
+/* the parameter sets of all blocks, as rocrand_make_constant lays them out in device memory */
+struct mtgp32_params
+{
+    unsigned int pos_tbl[MTGP_BN_MAX];
+    unsigned int param_tbl[MTGP_BN_MAX][MTGP_TS];
+    unsigned int temper_tbl[MTGP_BN_MAX][MTGP_TS];
+    unsigned int single_temper_tbl[MTGP_BN_MAX][MTGP_TS];
+    unsigned int sh1_tbl[MTGP_BN_MAX];
+    unsigned int sh2_tbl[MTGP_BN_MAX];
+    unsigned int mask[1];
+};
+
+struct mtgp32_state
+{
+    int          offset;
+    int          id;
+    unsigned int status[MTGP_STATE];
+};
+
+struct rocrand_state_mtgp32
+{
+    mtgp32_state m_state;
+    unsigned int pos_tbl;
+    unsigned int param_tbl[MTGP_TS];
+    unsigned int temper_tbl[MTGP_TS];
+    unsigned int sh1_tbl;
+    unsigned int sh2_tbl;
+    unsigned int single_temper_tbl[MTGP_TS];
+    unsigned int mask;
+
+    ROCRAND_B200_FN unsigned int recursion(unsigned int x1, unsigned int x2, unsigned int y) const
+    {
+        unsigned int x = (x1 & mask) ^ x2;
+        x ^= x << sh1_tbl;
+        y = x ^ (y >> sh2_tbl);
+        return y ^ param_tbl[y & 0x0f];
+    }
+    ROCRAND_B200_FN unsigned int temper(unsigned int v, unsigned int t) const
+    {
+        t ^= t >> 16;
+        t ^= t >> 8;
+        return v ^ temper_tbl[t & 0x0f];
+    }
+#if defined(__CUDACC__)
+    // every thread of the block, together
+    __device__ __forceinline__ unsigned int next()
+    {
+        const unsigned int t = threadIdx.x;
+        const int          k = m_state.offset;
+        const unsigned int r = recursion(m_state.status[(t + k) & MTGP_MASK], m_state.status[(t + k + 1) & MTGP_MASK],
+                                         m_state.status[(t + k + pos_tbl) & MTGP_MASK]);
+        m_state.status[(t + k + MTGP_N) & MTGP_MASK] = r;
+        const unsigned int o = temper(r, m_state.status[(t + k + pos_tbl - 1) & MTGP_MASK]);
+        __syncthreads();
+        if(t == 0)
+            m_state.offset = (m_state.offset + blockDim.x) & MTGP_MASK;
+        __syncthreads();
+        return o;
+    }
+#endif
+};
+
+namespace rocrand_b200_detail
+{
+// the seeding of one block's ring (rocrand_mtgp32.h:154-177): a fill byte from the tables,
+// the seed and a hidden word, then the Knuth-style recurrence over the 351 words
+inline void mtgp32_seed_ring(unsigned int array[], const mtgp32_fast_params* para, unsigned int seed)
+{
+    const int    size   = para->mexp / 32 + 1;
+    unsigned int hidden = para->tbl[4] ^ (para->tbl[8] << 16);
+    unsigned int tmp    = hidden;
+    tmp += tmp >> 16;
+    tmp += tmp >> 8;
+    memset(array, tmp & 0xff, sizeof(unsigned int) * size);
+    array[0] = seed;
+    array[1] = hidden;
+    for(int i = 1; i < size; i++)
+        array[i] ^= 1812433253u * (array[i - 1] ^ (array[i - 1] >> 30)) + static_cast<unsigned int>(i);
+}
+} // namespace rocrand_b200_detail
+
+/* Fills n states (device memory) for n blocks from parameter sets params[0..n) and seed
+ * (rocrand_mtgp32.h:394-430): block i gets set i and seed (uint)(seed ^ seed >> 32) + i + 1. */
+__host__ inline rocrand_status rocrand_make_state_mtgp32(rocrand_state_mtgp32* state, mtgp32_fast_params params[],
+                                                         int n, unsigned long long seed)
+{
+    rocrand_state_mtgp32* h = static_cast<rocrand_state_mtgp32*>(malloc(sizeof(rocrand_state_mtgp32) * n));
+    seed                    = seed ^ (seed >> 32);
+    if(h == NULL)
+        return ROCRAND_STATUS_ALLOCATION_FAILED;
+    for(int i = 0; i < n; i++)
+    {
+        rocrand_b200_detail::mtgp32_seed_ring(h[i].m_state.status, &params[i],
+                                              static_cast<unsigned int>(seed) + i + 1);
+        h[i].m_state.offset = 0;
+        h[i].m_state.id     = i;
+        h[i].pos_tbl        = params[i].pos;
+        h[i].sh1_tbl        = params[i].sh1;
+        h[i].sh2_tbl        = params[i].sh2;
+        h[i].mask           = params[0].mask;
+        for(int j = 0; j < MTGP_TS; j++)
+        {
+            h[i].param_tbl[j]         = params[i].tbl[j];
+            h[i].temper_tbl[j]        = params[i].tmp_tbl[j];
+            h[i].single_temper_tbl[j] = params[i].flt_tmp_tbl[j];
+        }
+    }
+    const cudaError_t e = cudaMemcpy(state, h, sizeof(rocrand_state_mtgp32) * n, cudaMemcpyDefault);
+    free(h);
+    return e == cudaSuccess ? ROCRAND_STATUS_SUCCESS : ROCRAND_STATUS_ALLOCATION_FAILED;
+}
+
+/* Lays the parameter sets of all MTGP_BN_MAX blocks out in p (device memory), for
+ * rocrand_mtgp32_set_params (rocrand_mtgp32.h:432-500). */
+__host__ inline rocrand_status rocrand_make_constant(const mtgp32_fast_params params[], mtgp32_params* p)
+{
+    mtgp32_params* h = static_cast<mtgp32_params*>(malloc(sizeof(mtgp32_params)));
+    if(h == NULL)
+        return ROCRAND_STATUS_ALLOCATION_FAILED;
+    h->mask[0] = params[0].mask;
+    for(int i = 0; i < MTGP_BN_MAX; i++)
+    {
+        h->pos_tbl[i] = params[i].pos;
+        h->sh1_tbl[i] = params[i].sh1;
+        h->sh2_tbl[i] = params[i].sh2;
+        for(int j = 0; j < MTGP_TS; j++)
+        {
+            h->param_tbl[i][j]         = params[i].tbl[j];
+            h->temper_tbl[i][j]        = params[i].tmp_tbl[j];
+            h->single_temper_tbl[i][j] = params[i].flt_tmp_tbl[j];
+        }
+    }
+    const cudaError_t e = cudaMemcpy(p, h, sizeof(mtgp32_params), cudaMemcpyHostToDevice);
+    free(h);
+    return e == cudaSuccess ? ROCRAND_STATUS_SUCCESS : ROCRAND_STATUS_ALLOCATION_FAILED;
+}
+
+#if defined(__CUDACC__)
+/* Block-cooperative copy of a state (e.g. from global into shared memory). */
+__device__ __forceinline__ void rocrand_mtgp32_block_copy(rocrand_state_mtgp32* src, rocrand_state_mtgp32* dest)
+{
+    const unsigned int t = threadIdx.x;
+    for(unsigned int i = t; i < MTGP_STATE; i += blockDim.x)
+        dest->m_state.status[i] = src->m_state.status[i];
+    if(t == 0)
+    {
+        dest->m_state.offset = src->m_state.offset;
+        dest->m_state.id     = src->m_state.id;
+        dest->pos_tbl        = src->pos_tbl;
+        dest->sh1_tbl        = src->sh1_tbl;
+        dest->sh2_tbl        = src->sh2_tbl;
+        dest->mask           = src->mask;
+    }
+    if(t < MTGP_TS)
+    {
+        dest->param_tbl[t]         = src->param_tbl[t];
+        dest->temper_tbl[t]        = src->temper_tbl[t];
+        dest->single_temper_tbl[t] = src->single_temper_tbl[t];
+    }
+    __syncthreads();
+}
+/* Takes the state's parameter set, number m_state.id, from a rocrand_make_constant table. */
+__device__ __forceinline__ void rocrand_mtgp32_set_params(rocrand_state_mtgp32* state, mtgp32_params* params)
+{
+    const int id   = state->m_state.id;
+    state->pos_tbl = params->pos_tbl[id];
+    state->sh1_tbl = params->sh1_tbl[id];
+    state->sh2_tbl = params->sh2_tbl[id];
+    state->mask    = params->mask[0];
+    for(int j = 0; j < MTGP_TS; j++)
+    {
+        state->param_tbl[j]         = params->param_tbl[id][j];
+        state->temper_tbl[j]        = params->temper_tbl[id][j];
+        state->single_temper_tbl[j] = params->single_temper_tbl[id][j];
+    }
+}
+#endif
 
 /* ThreeFry states (rocrand_threefry{2,4}_impl.h, rocrand_threefry{2x32,2x64,4x32,4x64}_20.h):
  * counter and key vectors of N words of type T, the current block and the position in it. */
@@ -2193,5 +2407,78 @@ ROCRAND_B200_QUASI_DISCRETE(rocrand_state_sobol64)
 ROCRAND_B200_QUASI_DISCRETE(rocrand_state_scrambled_sobol32)
 ROCRAND_B200_QUASI_DISCRETE(rocrand_state_scrambled_sobol64)
 #undef ROCRAND_B200_QUASI_DISCRETE
+
+// =======================================================================================
+// MTGP32: every function is called by all threads of the block together.
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ unsigned int rocrand(rocrand_state_mtgp32* state)
+{
+    return state->next();
+}
+__device__ __forceinline__ float rocrand_uniform(rocrand_state_mtgp32* state)
+{
+    return rocrand_b200_detail::to_float(rocrand(state));
+}
+__device__ __forceinline__ double rocrand_uniform_double(rocrand_state_mtgp32* state)
+{
+    return rocrand_b200_detail::to_double(rocrand(state));
+}
+__device__ __forceinline__ float rocrand_normal(rocrand_state_mtgp32* state)
+{
+    return rocrand_b200_detail::normal_inv(rocrand(state));
+}
+__device__ __forceinline__ float2 rocrand_normal2(rocrand_state_mtgp32* state)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    return rocrand_b200_detail::box_muller(a, b);
+}
+__device__ __forceinline__ double rocrand_normal_double(rocrand_state_mtgp32* state)
+{
+    return rocrand_b200_detail::normal_inv_double(rocrand(state));
+}
+__device__ __forceinline__ uint4 rocrand_b200_mtgp32_quad(rocrand_state_mtgp32* state)
+{
+    const unsigned int a = rocrand(state);
+    const unsigned int b = rocrand(state);
+    const unsigned int c = rocrand(state);
+    const unsigned int d = rocrand(state);
+    return make_uint4(a, b, c, d);
+}
+__device__ __forceinline__ double2 rocrand_normal_double2(rocrand_state_mtgp32* state)
+{
+    return rocrand_b200_detail::box_muller_double(rocrand_b200_mtgp32_quad(state));
+}
+__device__ __forceinline__ float rocrand_log_normal(rocrand_state_mtgp32* state, float mean, float stddev)
+{
+    float r = rocrand_b200_detail::normal_inv(rocrand(state));
+    return expf(mean + (stddev * r));
+}
+__device__ __forceinline__ float2 rocrand_log_normal2(rocrand_state_mtgp32* state, float mean, float stddev)
+{
+    const float2 r = rocrand_normal2(state);
+    return float2{expf(mean + (stddev * r.x)), expf(mean + (stddev * r.y))};
+}
+__device__ __forceinline__ double rocrand_log_normal_double(rocrand_state_mtgp32* state, double mean, double stddev)
+{
+    double r = rocrand_b200_detail::normal_inv_double(rocrand(state));
+    return exp(mean + (stddev * r));
+}
+__device__ __forceinline__ double2 rocrand_log_normal_double2(rocrand_state_mtgp32* state, double mean, double stddev)
+{
+    const double2 r = rocrand_b200_detail::box_muller_double(rocrand_b200_mtgp32_quad(state));
+    return double2{exp(mean + (stddev * r.x)), exp(mean + (stddev * r.y))};
+}
+__device__ __forceinline__ unsigned int rocrand_poisson(rocrand_state_mtgp32* state, double lambda)
+{
+    return rocrand_b200_detail::poisson_inversion(state, lambda);
+}
+__device__ __forceinline__ unsigned int rocrand_discrete(rocrand_state_mtgp32*               state,
+                                                         const rocrand_discrete_distribution discrete_distribution)
+{
+    return rocrand_b200_detail::alias_pick(rocrand(state), *discrete_distribution);
+}
+#endif
 
 #endif /* ROCRAND_KERNEL_H_ */

@@ -11,6 +11,7 @@
 // 32-byte slot: out[(t * calls + c) * 32].  A function an engine does not have stores
 // nothing and the call returns 1; a launch error returns 2.
 #include <rocrand/rocrand_kernel.h>
+#include <rocrand/rocrand_mtgp32_11213.h>
 
 #include <cuda_runtime.h>
 
@@ -284,7 +285,57 @@ __global__ void run_quasi(Args a, int* unsupported, bool scrambled)
             *unsupported = 1;
 }
 
+// MTGP32: one state per block copied into shared memory, every thread calling together;
+// with func 28 the parameter set is taken again from a rocrand_make_constant table first
+__global__ void run_mtgp32(Args a, int* unsupported, rocrand_state_mtgp32* states, mtgp32_params* consts)
+{
+    __shared__ rocrand_state_mtgp32 s;
+    rocrand_mtgp32_block_copy(&states[blockIdx.x], &s);
+    int func = a.func;
+    if(func == 28)
+    {
+        if(threadIdx.x == 0)
+            rocrand_mtgp32_set_params(&s, consts);
+        __syncthreads();
+        func = 0;
+    }
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    for(int c = 0; c < a.calls; c++)
+        if(!call(&s, func, c, a, a.out + (static_cast<size_t>(t) * a.calls + c) * 32))
+            *unsupported = 1;
+}
+
 } // namespace
+
+// devapi_run_mtgp32: `blocks` blocks of 256 threads, states made by rocrand_make_state_mtgp32
+// from the published parameter sets and `seed`.
+extern "C" int devapi_run_mtgp32(int func, unsigned long long seed, int blocks, int calls, double p0, double p1,
+                                 const void* dist, void* out)
+{
+    Args a{func, calls, p0, p1, seed, nullptr, 0, static_cast<const rocrand_discrete_distribution_st*>(dist),
+           static_cast<unsigned char*>(out)};
+    int*                  flag   = nullptr;
+    rocrand_state_mtgp32* states = nullptr;
+    mtgp32_params*        consts = nullptr;
+    int                   rc     = 2;
+    if(cudaMalloc(&flag, sizeof(int)) == cudaSuccess
+       && cudaMalloc(&states, sizeof(rocrand_state_mtgp32) * blocks) == cudaSuccess
+       && cudaMalloc(&consts, sizeof(mtgp32_params)) == cudaSuccess
+       && rocrand_make_state_mtgp32(states, mtgp32dc_params_fast_11213, blocks, seed) == ROCRAND_STATUS_SUCCESS
+       && rocrand_make_constant(mtgp32dc_params_fast_11213, consts) == ROCRAND_STATUS_SUCCESS)
+    {
+        cudaMemset(flag, 0, sizeof(int));
+        run_mtgp32<<<blocks, 256>>>(a, flag, states, consts);
+        int unsupported = 0;
+        if(cudaDeviceSynchronize() == cudaSuccess
+           && cudaMemcpy(&unsupported, flag, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
+            rc = unsupported ? 1 : 0;
+    }
+    cudaFree(flag);
+    cudaFree(states);
+    cudaFree(consts);
+    return rc;
+}
 
 extern "C" int devapi_run(int engine, int func, unsigned long long seed, int threads, int calls, double p0,
                           double p1, const void* vec, unsigned long long scramble, const void* dist, void* out)

@@ -49,6 +49,8 @@ def _load(path):
     lib.devapi_run.argtypes = [c_int, c_int, c_ulonglong, c_int, c_int, c_double, c_double, c_void_p,
                                c_ulonglong, c_void_p, c_void_p]
     lib.devapi_run.restype = c_int
+    lib.devapi_run_mtgp32.argtypes = [c_int, c_ulonglong, c_int, c_int, c_double, c_double, c_void_p, c_void_p]
+    lib.devapi_run_mtgp32.restype = c_int
     return lib
 
 
@@ -122,4 +124,28 @@ def test_device_api_equals_reference(env, engine, func, p0, p1):
     if sr == 1:
         pytest.skip("the reference has no %s for %s" % (func, engine))
     assert so == 0, "the reference has %s for %s, this library does not" % (func, engine)
+    assert np.array_equal(vo, vr), np.flatnonzero(vo != vr)[:8]
+
+
+MTGP_BLOCKS = 37
+
+
+@pytest.mark.parametrize("func,p0,p1", CASES + [("set_params", 0, 0)], ids=lambda x: str(x))
+def test_mtgp32_block_api_equals_reference(env, func, p0, p1):
+    """rocrand_state_mtgp32: states from rocrand_make_state_mtgp32 (published parameter sets),
+    block-copied to shared memory, every thread of the block calling together."""
+    import torch
+    ours, ref, _, _, dist = env
+    f = 28 if func == "set_params" else FUNCS[func]
+    outs = []
+    for lib in (ours, ref):
+        out = torch.zeros(MTGP_BLOCKS * 256 * CALLS * 32, dtype=torch.uint8, device="cuda")
+        st = lib.devapi_run_mtgp32(f, 0xC0FFEE1234, MTGP_BLOCKS, CALLS, float(p0), float(p1), dist.value,
+                                   out.data_ptr())
+        outs.append((st, out.cpu().numpy()))
+    (so, vo), (sr, vr) = outs
+    assert so != 2 and sr != 2, (so, sr)
+    if sr == 1:
+        pytest.skip("the reference has no %s for MTGP32" % func)
+    assert so == 0
     assert np.array_equal(vo, vr), np.flatnonzero(vo != vr)[:8]
