@@ -2,7 +2,7 @@
 //
 // Each functor reproduces one host functor of the reference (library/src/rng/distribution/
 // *.hpp) together with the scalar conversion it calls in the *host* branch of
-// library/include/rocrand/rocrand_{uniform,normal,discrete}.h, because parity is judged
+// library/include/rocrand/rocrand_{uniform,normal,discrete}.h, because parity is defined
 // against the reference's host generators.  Every rounding step is written with an
 // explicit _rn intrinsic: a product is fused into an FMA only where it is exact (scaling
 // by a power of two), so the device rounds exactly where the x86-64 host does.
