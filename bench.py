@@ -293,7 +293,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_batched:
         del out
         torch.cuda.empty_cache()
-        batched = batched_leg(lib, args.full_configs)
+        batched = batched_leg(lib, not args.quick_batched)
         torch.cuda.empty_cache()
         serving = serving_leg(lib, args.full_configs)
 
@@ -387,11 +387,11 @@ def _entry_args(d, p0, p1):
 
 
 def batched_leg(lib, full):
-    """Config 4: 4096 Philox4x32-10 + 4096 XORWOW fresh generators (seed_i = splitmix64(i),
+    """Batched fill: 4096 Philox4x32-10 + 4096 XORWOW fresh generators (seed_i = splitmix64(i),
     offset 0), sizes log-uniform in [2^10, 2^24] (numpy PCG64 seed 42), 50% uniform fp32 /
     30% normal fp32 / 20% Poisson lambda=4; one persistent launch replayed from a CUDA graph
     versus one plain call per generator (set_seed + generate, so every pass writes the same
-    values).  Without --full-configs a quarter of the requests (1024 + 1024)."""
+    values).  With --quick-batched a quarter of the requests (1024 + 1024)."""
     import numpy as np
     import torch
     import rocrand_b200 as rb
@@ -472,7 +472,7 @@ def batched_leg(lib, full):
 
 
 def serving_leg(lib, full):
-    """Config 5: Poisson arrivals at 1k-50k req/s over 64 handles (16 each of Philox,
+    """Serving: Poisson arrivals at 1k-50k req/s over 64 handles (16 each of Philox,
     XORWOW, MRG32k3a, Sobol32; states resident), sizes log-uniform in [2^8, 2^26], dtypes
     uniform over fp32 / fp64 / uint32, a 64 GB output budget; the continuous-batching server
     and the plain per-request server replay the same trace.  Also a saturated trace (every
@@ -660,8 +660,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="", help="gen:dist[:param],... subset of the sweep")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-fill and serving legs")
-    ap.add_argument("--full-configs", action="store_true",
-                    help="batched fill with 4096+4096 generators, serving with 10^5 requests per rate")
+    ap.add_argument("--full-configs", action="store_true", help="serving with 10^5 requests per rate")
+    ap.add_argument("--quick-batched", action="store_true",
+                    help="batched-fill leg on 1024 + 1024 generators instead of 4096 + 4096")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
