@@ -74,7 +74,7 @@ __device__ __forceinline__ void with_plain_functor(const BatchReq& r, Body&& bod
             if(r.huge)
                 body(FnPoissonHuge{r.sqrt_lambda, r.lambda});
             else
-                body(FnPoisson{r.prob, r.alias, r.tsize, r.toff});
+                body(FnPoisson{r.thr, r.alias, r.tsize, r.toff});
             break;
     }
 }
@@ -93,7 +93,7 @@ __device__ __forceinline__ void with_mrg_functor(const BatchReq& r, Body&& body)
             if(r.huge)
                 body(FnMrgPoissonHuge<N>{r.sqrt_lambda, r.lambda});
             else
-                body(FnMrgRemap<N, FnPoisson>{FnPoisson{r.prob, r.alias, r.tsize, r.toff}});
+                body(FnMrgRemap<N, FnPoisson>{FnPoisson{r.thr, r.alias, r.tsize, r.toff}});
             break;
     }
 }
@@ -457,6 +457,7 @@ rocrand_status batch_set_dist(BatchReq& r, uint32_t dist, double p0, double p1, 
     r.mean   = static_cast<float>(p0);
     r.stddev = static_cast<float>(p1);
     r.prob   = nullptr;
+    r.thr    = nullptr;
     r.alias  = nullptr;
     r.cdf    = nullptr;
     r.tsize = r.toff = r.huge = 0;
@@ -470,6 +471,7 @@ rocrand_status batch_set_dist(BatchReq& r, uint32_t dist, double p0, double p1, 
         if(st != ROCRAND_STATUS_SUCCESS)
             return st;
         r.prob        = dp.prob;
+        r.thr         = dp.thr;
         r.alias       = dp.alias;
         r.cdf         = dp.cdf;
         r.tsize       = dp.size;

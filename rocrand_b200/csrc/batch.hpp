@@ -61,6 +61,7 @@ struct BatchReq
     // distribution
     float         mean, stddev;
     const double* prob;
+    const unsigned long long* thr; // packed alias entries (poisson.hpp alias_entry)
     const uint32_t* alias;
     const double* cdf;
     uint32_t      tsize, toff, huge;

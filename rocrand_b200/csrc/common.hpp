@@ -43,6 +43,7 @@ struct DistParams
     uint16_t mean_h = 0, std_h = 0x3c00;
     // Poisson: alias table (device pointers) or the normal approximation above 4000.
     const double*   prob        = nullptr;
+    const unsigned long long* thr = nullptr; // packed alias entries (poisson.hpp alias_entry)
     const uint32_t* alias       = nullptr;
     const double*   cdf         = nullptr;
     uint32_t        size        = 0;

@@ -14,6 +14,7 @@
 // library's is itself correctly rounded.
 #pragma once
 
+#include <type_traits>
 #include "common.hpp"
 #include "precise_math.cuh"
 
@@ -131,6 +132,19 @@ __device__ __forceinline__ uint32_t alias_lookup(uint32_t r, uint32_t size, uint
     const double   y   = __dsub_rn(nx, fnx);
     const uint32_t i   = __double2uint_rz(fnx);
     return offset + (y < prob[i] ? i : alias[i]);
+}
+
+// The same pick from packed integer entries (poisson.hpp alias_entry: threshold in the low
+// 33 bits, alias above): i = (size r) >> 32, entry i when the low word of size r is below
+// the threshold.  One 8-byte read, no conversion or fp64 operation.
+__device__ __forceinline__ uint32_t alias_lookup_packed(uint32_t r, uint32_t size, uint32_t offset,
+                                                        const unsigned long long* tab)
+{
+    const unsigned long long p  = static_cast<unsigned long long>(size) * r;
+    const uint32_t           i  = static_cast<uint32_t>(p >> 32);
+    const unsigned long long e  = tab[i];
+    const unsigned long long lo = p & 0xffffffffull;
+    return offset + (lo < (e & 0x1ffffffffull) ? i : static_cast<uint32_t>(e >> 33));
 }
 
 // poisson.hpp:80-108 poisson_distribution_huge: round(sqrt(lambda) * N + lambda).
@@ -292,12 +306,12 @@ struct FnPoisson
     using T                      = uint32_t;
     static constexpr unsigned iw = 1, ow = 1;
     static constexpr bool     kTable = true;
-    const double*             prob;
-    const uint32_t*           alias;
+    const unsigned long long* prob;  // packed entries (alias_entry), not probabilities
+    const uint32_t*           alias; // unused: the aliases are packed with the thresholds
     uint32_t                  size, offset;
     __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
     {
-        out[0] = alias_lookup(in[0], size, offset, prob, alias);
+        out[0] = alias_lookup_packed(in[0], size, offset, prob);
     }
 };
 
@@ -639,18 +653,24 @@ __device__ __forceinline__ F stage_table(const F& fw, unsigned char* smem)
     if constexpr(has_table<F>::value)
     {
         const auto& f = table_of<F>::get(fw);
-        double*   p = reinterpret_cast<double*>(smem);
-        uint32_t* a = reinterpret_cast<uint32_t*>(smem + sizeof(double) * f.size);
+        using E       = typename std::remove_cv<typename std::remove_pointer<decltype(f.prob)>::type>::type;
+        static_assert(sizeof(E) == 8, "8-byte table entries");
+        // packed entries (FnPoisson) carry their aliases; Fn64Poisson has a separate array
+        constexpr bool packed = std::is_same<E, unsigned long long>::value;
+        E*        p = reinterpret_cast<E*>(smem);
+        uint32_t* a = reinterpret_cast<uint32_t*>(smem + sizeof(E) * f.size);
         for(uint32_t i = threadIdx.x; i < f.size; i += blockDim.x)
         {
             p[i] = f.prob[i];
-            a[i] = f.alias[i];
+            if constexpr(!packed)
+                a[i] = f.alias[i];
         }
         __syncthreads();
         F     g  = fw;
         auto& gt = table_of<F>::get(g);
         gt.prob  = p;
-        gt.alias = a;
+        if constexpr(!packed)
+            gt.alias = a;
         return g;
     }
     else
@@ -663,7 +683,12 @@ template<class F>
 inline size_t table_smem_bytes(const F& f)
 {
     if constexpr(has_table<F>::value)
-        return (size_t)table_of<F>::get(f).size * (sizeof(double) + sizeof(uint32_t));
+    {
+        const auto& t = table_of<F>::get(f);
+        using E       = typename std::remove_cv<typename std::remove_pointer<decltype(t.prob)>::type>::type;
+        constexpr bool packed = std::is_same<E, unsigned long long>::value;
+        return (size_t)t.size * (sizeof(E) + (packed ? 0 : sizeof(uint32_t)));
+    }
     else
         return 0;
 }
@@ -694,7 +719,7 @@ inline rocrand_status with_functor(Dist d, const DistParams& p, Body&& body)
         case Dist::POISSON:
             if(p.huge)
                 return body(FnPoissonHuge{p.sqrt_lambda, p.lambda});
-            return body(FnPoisson{p.prob, p.alias, p.size, p.offset});
+            return body(FnPoisson{p.thr, p.alias, p.size, p.offset});
         default: return ROCRAND_STATUS_TYPE_ERROR;
     }
 }
@@ -722,7 +747,7 @@ inline rocrand_status with_functor_mrg(Dist d, const DistParams& p, Body&& body)
         case Dist::POISSON:
             if(p.huge)
                 return body(FnMrgPoissonHuge<N>{p.sqrt_lambda, p.lambda});
-            return body(FnMrgRemap<N, FnPoisson>{FnPoisson{p.prob, p.alias, p.size, p.offset}});
+            return body(FnMrgRemap<N, FnPoisson>{FnPoisson{p.thr, p.alias, p.size, p.offset}});
         default: return ROCRAND_STATUS_TYPE_ERROR;
     }
 }

@@ -30,7 +30,8 @@ namespace rb200
 
 constexpr uint32_t kNoallocTableEntries = 4096;
 
-static __device__ __align__(256) double   g_noalloc_prob[kNoallocTableEntries];
+// packed alias entries (poisson.hpp alias_entry); the alias array stays for the layout
+static __device__ __align__(256) unsigned long long g_noalloc_thr[kNoallocTableEntries];
 static __device__ __align__(256) uint32_t g_noalloc_alias[kNoallocTableEntries];
 
 namespace
@@ -38,7 +39,7 @@ namespace
 
 struct NoallocScratch
 {
-    double*   prob  = nullptr;
+    unsigned long long* thr = nullptr;
     uint32_t* alias = nullptr;
 };
 
@@ -51,14 +52,14 @@ rocrand_status scratch_for_current_device(NoallocScratch& out)
     if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
         return ROCRAND_STATUS_INTERNAL_ERROR;
     std::lock_guard<std::mutex> lock(mu);
-    if(cache[dev].prob == nullptr)
+    if(cache[dev].thr == nullptr)
     {
         void* p = nullptr;
         void* a = nullptr;
-        if(cudaGetSymbolAddress(&p, g_noalloc_prob) != cudaSuccess
+        if(cudaGetSymbolAddress(&p, g_noalloc_thr) != cudaSuccess
            || cudaGetSymbolAddress(&a, g_noalloc_alias) != cudaSuccess)
             return ROCRAND_STATUS_INTERNAL_ERROR;
-        cache[dev].prob  = static_cast<double*>(p);
+        cache[dev].thr   = static_cast<unsigned long long*>(p);
         cache[dev].alias = static_cast<uint32_t*>(a);
     }
     out = cache[dev];
@@ -70,6 +71,7 @@ struct HostTable
 {
     double   p[kNoallocTableEntries];
     double   prob[kNoallocTableEntries];
+    unsigned long long thr[kNoallocTableEntries];
     uint32_t alias[kNoallocTableEntries];
     uint32_t small[kNoallocTableEntries];
     uint32_t large[kNoallocTableEntries];
@@ -150,6 +152,8 @@ bool build_table(double lambda, uint32_t& size, uint32_t& offset)
         t.prob[t.small[i]] = 1.0;
     for(uint32_t i = 0; i < nl; i++)
         t.prob[t.large[i]] = 1.0;
+    for(uint32_t i = 0; i < size; i++)
+        t.thr[i] = alias_entry(t.prob[i], t.alias[i]);
     return true;
 }
 
@@ -190,14 +194,14 @@ extern "C" rocrand_status ROCRANDAPI
             return ROCRAND_STATUS_SUCCESS;
         // Pageable sources: each copy returns once the source has been read, so the
         // per-thread staging can be reused by the next call.
-        if(cudaMemcpyAsync(s.prob, t_table.prob, sizeof(double) * size, cudaMemcpyHostToDevice, stream)
+        if(cudaMemcpyAsync(s.thr, t_table.thr, sizeof(unsigned long long) * size, cudaMemcpyHostToDevice, stream)
                != cudaSuccess
            || cudaMemcpyAsync(s.alias, t_table.alias, sizeof(uint32_t) * size,
                               cudaMemcpyHostToDevice, stream)
                   != cudaSuccess)
             return ROCRAND_STATUS_INTERNAL_ERROR;
         p.huge   = 0;
-        p.prob   = s.prob;
+        p.thr    = s.thr;
         p.alias  = s.alias;
         p.size   = size;
         p.offset = table_offset;

@@ -242,7 +242,7 @@ rocrand_status philox_poisson_with_table(unsigned long long seed, unsigned long 
     a.vec    = a.data + mis * sizeof(unsigned int);
     if(p.huge)
         return launch_philox(a, FnPoissonHuge{p.sqrt_lambda, p.lambda}, stream);
-    return launch_philox(a, FnPoisson{p.prob, p.alias, p.size, p.offset}, stream);
+    return launch_philox(a, FnPoisson{p.thr, p.alias, p.size, p.offset}, stream);
 }
 
 rocrand_status PhiloxGenerator::batch_descriptor(uint32_t dist, double p0, double p1, void* data,

@@ -117,9 +117,11 @@ PoissonCache::~PoissonCache()
         cudaEventDestroy(m_upload);
     }
     cudaFree(d_prob);
+    cudaFree(d_thr);
     cudaFree(d_alias);
     cudaFree(d_cdf);
     cudaFreeHost(h_prob);
+    cudaFreeHost(h_thr);
     cudaFreeHost(h_alias);
     cudaFreeHost(h_cdf);
 }
@@ -137,9 +139,11 @@ rocrand_status PoissonCache::get(double lambda, cudaStream_t stream, bool with_c
     {
         m_cap = poisson_capacity(kPoissonHugeLambda);
         if(cudaMalloc(&d_prob, m_cap * sizeof(double)) != cudaSuccess
+           || cudaMalloc(&d_thr, m_cap * sizeof(unsigned long long)) != cudaSuccess
            || cudaMalloc(&d_alias, m_cap * sizeof(uint32_t)) != cudaSuccess
            || cudaMalloc(&d_cdf, m_cap * sizeof(double)) != cudaSuccess
            || cudaMallocHost(&h_prob, m_cap * sizeof(double)) != cudaSuccess
+           || cudaMallocHost(&h_thr, m_cap * sizeof(unsigned long long)) != cudaSuccess
            || cudaMallocHost(&h_alias, m_cap * sizeof(uint32_t)) != cudaSuccess
            || cudaMallocHost(&h_cdf, m_cap * sizeof(double)) != cudaSuccess
            || cudaEventCreateWithFlags(&m_upload, cudaEventDisableTiming) != cudaSuccess)
@@ -156,10 +160,15 @@ rocrand_status PoissonCache::get(double lambda, cudaStream_t stream, bool with_c
         if(m_pending && cudaEventSynchronize(m_upload) != cudaSuccess)
             return ROCRAND_STATUS_INTERNAL_ERROR;
         std::memcpy(h_prob, t.prob.data(), t.size * sizeof(double));
+        for(uint32_t i = 0; i < t.size; i++)
+            h_thr[i] = alias_entry(t.prob[i], t.alias[i]);
         std::memcpy(h_alias, t.alias.data(), t.size * sizeof(uint32_t));
         std::memcpy(h_cdf, t.cdf.data(), t.size * sizeof(double));
         if(cudaMemcpyAsync(d_prob, h_prob, t.size * sizeof(double), cudaMemcpyHostToDevice, stream)
                != cudaSuccess
+           || cudaMemcpyAsync(d_thr, h_thr, t.size * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                              stream)
+                  != cudaSuccess
            || cudaMemcpyAsync(d_alias, h_alias, t.size * sizeof(uint32_t), cudaMemcpyHostToDevice,
                               stream)
                   != cudaSuccess
@@ -175,6 +184,7 @@ rocrand_status PoissonCache::get(double lambda, cudaStream_t stream, bool with_c
     }
     p.huge   = 0;
     p.prob   = d_prob;
+    p.thr    = d_thr;
     p.alias  = d_alias;
     p.cdf    = d_cdf;
     p.size   = m_size;

@@ -9,6 +9,7 @@
 
 #include "common.hpp"
 
+#include <cmath>
 #include <vector>
 
 namespace rb200
@@ -42,6 +43,21 @@ void build_cdf(const std::vector<double>& p, uint32_t size, std::vector<double>&
 // Builds the full table for lambda (prob, alias and cdf).
 void build_poisson_table(double lambda, HostPoissonTable& t);
 
+// The alias-table test of a 32-bit input r (discrete_alias, rocrand_discrete.h:38-63):
+// x = r 2^-32, nx = size x, y = nx - floor(nx), pick i = floor(nx) when y < prob[i].  With
+// r < 2^32 and size <= 4096 every step is exact, so i = (size r) >> 32 and y < prob[i] is
+// ((size r) mod 2^32) < prob[i] 2^32, i.e. the low word below ceil(prob[i] 2^32): the kernels
+// compare integers against these thresholds and pick the same entries.
+inline unsigned long long alias_threshold(double prob)
+{
+    return prob >= 1.0 ? (1ull << 32) : static_cast<unsigned long long>(std::ceil(std::ldexp(prob, 32)));
+}
+// The kernels' table entry: threshold (33 bits) and alias (the rest) in one 64-bit word.
+inline unsigned long long alias_entry(double prob, uint32_t alias)
+{
+    return alias_threshold(prob) | (static_cast<unsigned long long>(alias) << 33);
+}
+
 // Per-generator device cache of the table for the most recent lambda.
 class PoissonCache
 {
@@ -61,9 +77,11 @@ private:
     uint32_t     m_cap     = 0;
     uint32_t     m_size = 0, m_offset = 0;
     double*      d_prob  = nullptr;
+    unsigned long long* d_thr = nullptr; // packed alias entries (alias_entry)
     uint32_t*    d_alias = nullptr;
     double*      d_cdf   = nullptr;
     double*      h_prob  = nullptr; // pinned staging
+    unsigned long long* h_thr = nullptr;
     uint32_t*    h_alias = nullptr;
     double*      h_cdf   = nullptr;
     cudaEvent_t  m_upload = nullptr;
