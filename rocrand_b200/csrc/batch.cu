@@ -658,11 +658,13 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
     int dev = 0;
     if(cudaGetDevice(&dev) != cudaSuccess)
         return ROCRAND_STATUS_INTERNAL_ERROR;
+    // Device tables grow geometrically: cudaFree synchronises the whole device, which would
+    // serialise the server's streams if a table were resized for every batch.
     if(m_reqs.size() > m_cap || dev != m_device)
     {
         cudaFree(d_reqs);
         d_reqs = nullptr;
-        m_cap  = std::max<size_t>(m_reqs.size(), 1);
+        m_cap  = std::max<size_t>({m_reqs.size(), 2 * m_cap, 256});
         // descriptors followed by the tile counter
         if(cudaMalloc(&d_reqs, sizeof(BatchReq) * m_cap + 256) != cudaSuccess)
         {
@@ -681,13 +683,14 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
     {
         cudaFree(d_seq);
         d_seq = nullptr;
-        if(cudaMalloc(&d_seq, sizeof(uint32_t) * m_seq.size()) != cudaSuccess)
+        const size_t cap = std::max<size_t>({m_seq.size(), 2 * m_seq_cap, 2 * kXorwowSeqWords * 64});
+        if(cudaMalloc(&d_seq, sizeof(uint32_t) * cap) != cudaSuccess)
         {
             d_seq     = nullptr;
             m_seq_cap = 0;
             return ROCRAND_STATUS_ALLOCATION_FAILED;
         }
-        m_seq_cap = m_seq.size();
+        m_seq_cap = cap;
         if(m_exec)
         {
             cudaGraphExecDestroy(m_exec);
@@ -698,13 +701,14 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
     {
         cudaFree(d_tile_req);
         d_tile_req = nullptr;
-        if(cudaMalloc(&d_tile_req, sizeof(uint32_t) * m_tile_req.size()) != cudaSuccess)
+        const size_t cap = std::max<size_t>({m_tile_req.size(), 2 * m_tile_cap, size_t(1) << 16});
+        if(cudaMalloc(&d_tile_req, sizeof(uint32_t) * cap) != cudaSuccess)
         {
             d_tile_req = nullptr;
             m_tile_cap = 0;
             return ROCRAND_STATUS_ALLOCATION_FAILED;
         }
-        m_tile_cap = m_tile_req.size();
+        m_tile_cap = cap;
         if(m_exec)
         {
             cudaGraphExecDestroy(m_exec);

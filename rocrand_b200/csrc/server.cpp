@@ -244,6 +244,7 @@ public:
         ticket               = r->ticket;
         m_queue.push_back(r.get());
         m_reqs[ticket] = std::move(r);
+        m_last_submit  = now_s();
         m_cv.notify_all();
         return ROCRAND_STATUS_SUCCESS;
     }
@@ -332,33 +333,46 @@ private:
         }
     }
 
+    // One ordinary generate call for a request on `stream`.
+    rocrand_status plain_call(Request* r, cudaStream_t stream)
+    {
+        Handle& h = *r->h;
+        h.gen->set_stream(stream);
+        void*          out = m_pool + r->off;
+        rocrand_status st;
+        DistParams     dp;
+        switch(r->dist)
+        {
+            case BD_UINT: st = h.gen->generate(out, r->n, Dist::U32, dp); break;
+            case BD_FLOAT: st = h.gen->generate(out, r->n, Dist::F32, dp); break;
+            case BD_DOUBLE: st = h.gen->generate(out, r->n, Dist::F64, dp); break;
+            case BD_NORMAL_F:
+                dp.mean_f = static_cast<float>(r->p0);
+                dp.std_f  = static_cast<float>(r->p1);
+                st        = h.gen->generate(out, r->n, Dist::NORMAL_F32, dp);
+                break;
+            default: st = h.gen->generate_poisson(static_cast<unsigned int*>(out), r->n, r->p0); break;
+        }
+        return st;
+    }
+
     // Launches one batch (or, in plain mode, one ordinary call) of admitted requests.
     rocrand_status launch(std::vector<Request*>& reqs, int s)
     {
         cudaStream_t stream = m_streams[s];
+        if(!m_plain && reqs.size() == 1 && reqs[0]->dist != BD_POISSON)
+        {
+            // a batch of one: the ordinary call is the shorter launch.  (Poisson stays on the
+            // batch path, whose tables are shared across streams; a generator's own table
+            // would be refreshed on this stream while another stream may still read it.)
+            Handle& h = *reqs[0]->h;
+            if(h.stateful && h.last_pending)
+                cudaStreamWaitEvent(stream, h.last, 0);
+            return plain_call(reqs[0], stream);
+        }
         if(m_plain)
         {
-            Request* r = reqs[0];
-            Handle&  h = *r->h;
-            h.gen->set_stream(stream);
-            void*          out = m_pool + r->off;
-            rocrand_status st;
-            DistParams     dp;
-            switch(r->dist)
-            {
-                case BD_UINT: st = h.gen->generate(out, r->n, Dist::U32, dp); break;
-                case BD_FLOAT: st = h.gen->generate(out, r->n, Dist::F32, dp); break;
-                case BD_DOUBLE: st = h.gen->generate(out, r->n, Dist::F64, dp); break;
-                case BD_NORMAL_F:
-                    dp.mean_f = static_cast<float>(r->p0);
-                    dp.std_f  = static_cast<float>(r->p1);
-                    st        = h.gen->generate(out, r->n, Dist::NORMAL_F32, dp);
-                    break;
-                default:
-                    st = h.gen->generate_poisson(static_cast<unsigned int*>(out), r->n, r->p0);
-                    break;
-            }
-            return st;
+            return plain_call(reqs[0], stream);
         }
         // each stream reuses its own descriptor table: its previous batch is finished
         BatchPlan& plan = *m_plans[s];
@@ -425,7 +439,13 @@ private:
                         s = static_cast<int>(k);
                         break;
                     }
-            if(s >= 0 && !m_queue.empty())
+            // While a burst of submissions is arriving and a batch is already on the device,
+            // let a few more requests gather instead of launching tiny batches back to back
+            // (each launch costs its own descriptor upload): hold while fewer than
+            // kGatherRequests are queued and the last submission was under kGatherGap ago.
+            const bool gather = !m_plain && !inflight.empty() && m_queue.size() < kGatherRequests
+                                && now_s() - m_last_submit < kGatherGap;
+            if(s >= 0 && !m_queue.empty() && !gather)
             {
                 std::vector<Request*> reqs;
                 admit(reqs, m_plain ? 1 : 8192, m_plain ? m_budget : (size_t(8) << 30));
@@ -475,7 +495,9 @@ private:
         }
     }
 
-    static constexpr size_t       kPlainInFlight = 4096;
+    static constexpr size_t       kPlainInFlight  = 4096;
+    static constexpr size_t       kGatherRequests = 64;
+    static constexpr double       kGatherGap      = 20e-6; // seconds
     size_t                        m_budget;
     bool                          m_plain;
     unsigned                      m_nstreams = 1;
@@ -491,7 +513,8 @@ private:
     std::mutex                    m_mu;
     std::condition_variable       m_cv, m_done_cv;
     std::thread                   m_worker;
-    bool                          m_stop = false;
+    bool                          m_stop        = false;
+    double                        m_last_submit = 0.0;
 };
 
 } // namespace rb200
