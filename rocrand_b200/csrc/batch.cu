@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -565,6 +566,12 @@ BatchPlan::~BatchPlan()
 {
     if(m_exec)
         cudaGraphExecDestroy(m_exec);
+    if(m_staged)
+    {
+        cudaEventSynchronize(m_staged);
+        cudaEventDestroy(m_staged);
+    }
+    cudaFreeHost(h_stage);
     cudaFree(d_reqs);
     cudaFree(d_seq);
     cudaFree(d_tile_req);
@@ -636,6 +643,62 @@ rocrand_status BatchPlan::build(const void* requests, size_t count, cudaStream_t
         if(u.n == 0)
             continue;
         m_reqs.push_back(r);
+    }
+    return ROCRAND_STATUS_SUCCESS;
+}
+
+rocrand_status BatchPlan::reserve(size_t reqs, size_t tiles)
+{
+    int dev = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess)
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    if(reqs > m_cap || dev != m_device)
+    {
+        cudaFree(d_reqs);
+        d_reqs = nullptr;
+        m_cap  = 0;
+        if(cudaMalloc(&d_reqs, sizeof(BatchReq) * reqs + 256) != cudaSuccess)
+        {
+            d_reqs = nullptr;
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        }
+        m_cap    = reqs;
+        m_device = dev;
+        if(m_exec)
+        {
+            cudaGraphExecDestroy(m_exec);
+            m_exec = nullptr;
+        }
+    }
+    if(tiles > m_tile_cap)
+    {
+        cudaFree(d_tile_req);
+        d_tile_req = nullptr;
+        m_tile_cap = 0;
+        if(cudaMalloc(&d_tile_req, sizeof(uint32_t) * tiles) != cudaSuccess)
+        {
+            d_tile_req = nullptr;
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        }
+        m_tile_cap = tiles;
+    }
+    const size_t stage = sizeof(uint32_t) * tiles + sizeof(BatchReq) * reqs + 32;
+    if(stage > m_stage_cap)
+    {
+        cudaFreeHost(h_stage);
+        h_stage     = nullptr;
+        m_stage_cap = 0;
+        if(cudaHostAlloc(reinterpret_cast<void**>(&h_stage), stage, cudaHostAllocDefault) != cudaSuccess)
+        {
+            h_stage = nullptr;
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        }
+        m_stage_cap = stage;
+    }
+    if(m_staged == nullptr && cudaEventCreateWithFlags(&m_staged, cudaEventDisableTiming) != cudaSuccess)
+    {
+        m_staged = nullptr;
+        return ROCRAND_STATUS_INTERNAL_ERROR;
     }
     return ROCRAND_STATUS_SUCCESS;
 }
@@ -715,22 +778,49 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
             m_exec = nullptr;
         }
     }
-    if(!m_tile_req.empty()
-       && cudaMemcpyAsync(d_tile_req, m_tile_req.data(), sizeof(uint32_t) * m_tile_req.size(),
-                          cudaMemcpyHostToDevice, stream)
-              != cudaSuccess)
-        return ROCRAND_STATUS_INTERNAL_ERROR;
-    if(!m_seq.empty()
-       && cudaMemcpyAsync(d_seq, m_seq.data(), sizeof(uint32_t) * m_seq.size(), cudaMemcpyHostToDevice,
-                          stream)
-              != cudaSuccess)
-        return ROCRAND_STATUS_INTERNAL_ERROR;
     d_next = reinterpret_cast<unsigned long long*>(reinterpret_cast<unsigned char*>(d_reqs)
                                                    + sizeof(BatchReq) * m_cap);
-    if(!m_reqs.empty()
-       && cudaMemcpyAsync(d_reqs, m_reqs.data(), sizeof(BatchReq) * m_reqs.size(),
-                          cudaMemcpyHostToDevice, stream)
-              != cudaSuccess)
+    // the three tables go through one pinned buffer, which the previous upload's copies must
+    // have read before it is refilled (immediate in the server: a plan's last batch is done)
+    auto         up16   = [](size_t b) { return (b + 15) / 16 * 16; };
+    const size_t b_tile = sizeof(uint32_t) * m_tile_req.size();
+    const size_t b_seq  = sizeof(uint32_t) * m_seq.size();
+    const size_t b_reqs = sizeof(BatchReq) * m_reqs.size();
+    const size_t total  = up16(b_tile) + up16(b_seq) + b_reqs;
+    if(total == 0)
+        return ROCRAND_STATUS_SUCCESS;
+    if(m_staged == nullptr && cudaEventCreateWithFlags(&m_staged, cudaEventDisableTiming) != cudaSuccess)
+    {
+        m_staged = nullptr;
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    }
+    if(cudaEventSynchronize(m_staged) != cudaSuccess)
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    if(total > m_stage_cap)
+    {
+        const size_t cap = std::max<size_t>({total, 2 * m_stage_cap, size_t(1) << 20});
+        cudaFreeHost(h_stage);
+        h_stage     = nullptr;
+        m_stage_cap = 0;
+        if(cudaHostAlloc(reinterpret_cast<void**>(&h_stage), cap, cudaHostAllocDefault) != cudaSuccess)
+        {
+            h_stage = nullptr;
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        }
+        m_stage_cap = cap;
+    }
+    unsigned char* seq  = h_stage + up16(b_tile);
+    unsigned char* reqs = seq + up16(b_seq);
+    if(b_tile)
+        std::memcpy(h_stage, m_tile_req.data(), b_tile);
+    if(b_seq)
+        std::memcpy(seq, m_seq.data(), b_seq);
+    if(b_reqs)
+        std::memcpy(reqs, m_reqs.data(), b_reqs);
+    if((b_tile && cudaMemcpyAsync(d_tile_req, h_stage, b_tile, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+       || (b_seq && cudaMemcpyAsync(d_seq, seq, b_seq, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+       || (b_reqs && cudaMemcpyAsync(d_reqs, reqs, b_reqs, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+       || cudaEventRecord(m_staged, stream) != cudaSuccess)
         return ROCRAND_STATUS_INTERNAL_ERROR;
     return ROCRAND_STATUS_SUCCESS;
 }

@@ -101,6 +101,9 @@ public:
     void clear() { m_reqs.clear(); }
     // Serving batches (resident states, latency-bound mixes) take the serving tile sizes.
     void set_serving(bool serving) { m_serving = serving; }
+    // Allocates the device tables and the pinned staging buffer for batches of up to `reqs`
+    // requests and `tiles` tiles now, so that the first batches do not allocate.
+    rocrand_status reserve(size_t reqs, size_t tiles);
     // Assigns tiles and uploads the table on `stream`.
     rocrand_status upload(cudaStream_t stream);
     // Launches the persistent kernel (resets the tile counter first).
@@ -126,6 +129,11 @@ private:
     size_t                m_cap     = 0;
     cudaGraphExec_t       m_exec    = nullptr;
     int                   m_device  = -1;
+    // pinned copy of the three tables: from pageable memory cudaMemcpyAsync may hold the host
+    // until the stream reaches the copy, i.e. until the work it is queued behind has run
+    unsigned char*        h_stage     = nullptr;
+    size_t                m_stage_cap = 0;
+    cudaEvent_t           m_staged    = nullptr; // the last upload's copies have read h_stage
 };
 
 // Fills the distribution fields of a descriptor (Poisson tables are cached per lambda).

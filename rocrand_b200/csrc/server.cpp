@@ -157,6 +157,12 @@ public:
             m_streams.push_back(st);
             m_plans.emplace_back(new BatchPlan());
             m_plans.back()->set_serving(true);
+            // tables for a large batch now, not on the request path (allocation is slow and
+            // freeing a table to grow it waits for the whole device)
+            const rocrand_status rst
+                = m_plain ? ROCRAND_STATUS_SUCCESS : m_plans.back()->reserve(kMaxBatchRequests, size_t(1) << 20);
+            if(rst != ROCRAND_STATUS_SUCCESS)
+                return rst;
         }
         m_worker = std::thread([this] { loop(); });
         return ROCRAND_STATUS_SUCCESS;
@@ -448,7 +454,7 @@ private:
             if(s >= 0 && !m_queue.empty() && !gather)
             {
                 std::vector<Request*> reqs;
-                admit(reqs, m_plain ? 1 : 8192, m_plain ? m_budget : (size_t(8) << 30));
+                admit(reqs, m_plain ? 1 : kMaxBatchRequests, m_plain ? m_budget : (size_t(8) << 30));
                 if(!reqs.empty())
                 {
                     InFlight f;
@@ -495,6 +501,7 @@ private:
         }
     }
 
+    static constexpr size_t       kMaxBatchRequests = 8192;
     static constexpr size_t       kPlainInFlight  = 4096;
     static constexpr size_t       kGatherRequests = 64;
     static constexpr double       kGatherGap      = 20e-6; // seconds
