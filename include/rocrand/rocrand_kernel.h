@@ -58,9 +58,16 @@
 #define ROCRAND_SQRT2 (1.4142135f)
 #define ROCRAND_SQRT2_DOUBLE (1.4142135623730951)
 
+// default seeds (rocrand_philox4x32_10.h:73, rocrand_xorwow.h:35, rocrand_mrg32k3a.h:49,
+// rocrand_mrg31k3p.h:44, rocrand_lfsr113.h:33-42); the C++ wrapper's engines default to them
 #define ROCRAND_PHILOX4x32_DEFAULT_SEED 0xdeadbeefdeadbeefULL
+#define ROCRAND_XORWOW_DEFAULT_SEED 0ULL
 #define ROCRAND_MRG32K3A_DEFAULT_SEED 12345ULL
 #define ROCRAND_MRG31K3P_DEFAULT_SEED 12345ULL
+#define ROCRAND_LFSR113_DEFAULT_SEED_X 2
+#define ROCRAND_LFSR113_DEFAULT_SEED_Y 8
+#define ROCRAND_LFSR113_DEFAULT_SEED_Z 16
+#define ROCRAND_LFSR113_DEFAULT_SEED_W 128
 
 namespace rocrand_b200_detail
 {
