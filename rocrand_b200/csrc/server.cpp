@@ -13,6 +13,7 @@
 // taken in submission order from the generator's own state (batch_descriptor).
 // The plain mode runs the same admission and memory pool but issues one ordinary
 // generate call per request on one stream: the per-request baseline.
+#include "admission.hpp"
 #include "batch.hpp"
 #include "common.hpp"
 #include "generators.hpp"
@@ -248,7 +249,7 @@ public:
         r->t_submit          = t_arrival > 0 ? t_arrival : now_s();
         r->release_when_done = release_when_done;
         ticket               = r->ticket;
-        m_queue.push_back(r.get());
+        m_queue.push(r.get(), handle);
         m_reqs[ticket] = std::move(r);
         m_last_submit  = now_s();
         m_cv.notify_all();
@@ -287,43 +288,21 @@ public:
     }
 
 private:
-    // Takes queued requests in arrival order while output memory lasts; a request that
-    // does not fit stops admission (no overtaking), a stateful handle joins a batch once.
+    // Takes queued requests in arrival order while output memory lasts (admission.hpp: a
+    // request that does not fit stops admission, a stateful handle joins a batch once).
     void admit(std::vector<Request*>& out, size_t max_reqs, size_t max_bytes)
     {
-        std::vector<uint32_t> used, blocked;
-        size_t                bytes = 0;
-        auto                  it    = m_queue.begin();
-        auto has = [](const std::vector<uint32_t>& v, uint32_t x) {
-            return std::find(v.begin(), v.end(), x) != v.end();
-        };
-        while(it != m_queue.end() && out.size() < max_reqs)
-        {
-            Request*      r = *it;
-            const Handle& h = *r->h;
-            // a stateful handle joins a batch once; its later requests (and anything after a
-            // skipped request of the same handle) wait for the next batch, so each handle
-            // keeps its arrival order while other handles' requests go ahead
-            if(has(blocked, r->handle) || (h.stateful && has(used, r->handle)))
-            {
-                if(!has(blocked, r->handle))
-                    blocked.push_back(r->handle);
-                ++it;
-                continue;
-            }
-            if(!out.empty() && bytes + r->bytes > max_bytes)
-                break;
-            size_t off = 0;
-            if(!m_alloc.alloc(r->bytes, off))
-                break;
-            r->off   = off;
-            r->state = 1;
-            bytes += r->bytes;
-            if(h.stateful)
-                used.push_back(r->handle);
-            out.push_back(r);
-            it = m_queue.erase(it);
-        }
+        m_queue.admit(
+            out, max_reqs, max_bytes, [](const Request* r) { return r->h->stateful; },
+            [](const Request* r) { return r->bytes; },
+            [this](Request* r) {
+                size_t off = 0;
+                if(!m_alloc.alloc(r->bytes, off))
+                    return false;
+                r->off   = off;
+                r->state = 1;
+                return true;
+            });
     }
 
     void finish(Request* r, rocrand_status st)
@@ -514,7 +493,7 @@ private:
     std::vector<cudaStream_t>     m_streams;
     std::vector<std::unique_ptr<BatchPlan>> m_plans;
     std::deque<Handle>            m_handles;
-    std::deque<Request*>          m_queue;
+    AdmissionQueue<Request>       m_queue;
     std::unordered_map<unsigned long long, std::unique_ptr<Request>> m_reqs;
     unsigned long long            m_next_ticket = 0;
     std::mutex                    m_mu;
