@@ -444,6 +444,10 @@ public:
     {
         if(m_initialized)
             return ROCRAND_STATUS_SUCCESS;
+        // the Poisson tables are allocated here, as the reference's generators do in init(), so
+        // that a generate call recorded by a stream capture allocates nothing
+        if(m_poisson.reserve() != ROCRAND_STATUS_SUCCESS)
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
         const uint32_t* polys = device_jump_polys();
         if(polys == nullptr)
             return ROCRAND_STATUS_ALLOCATION_FAILED;

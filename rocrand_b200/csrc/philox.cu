@@ -150,6 +150,11 @@ rocrand_status PhiloxGenerator::init()
 {
     if(m_initialized)
         return ROCRAND_STATUS_SUCCESS;
+    // the Poisson tables are allocated here, as the reference's generators do in init(), so
+    // that a generate call recorded by a stream capture allocates nothing
+    const rocrand_status st = m_poisson.reserve();
+    if(st != ROCRAND_STATUS_SUCCESS)
+        return st;
     // seed(seed, subsequence 0, offset) (philox4x32_10.hpp:291-306, engine seed :134-141)
     m_pos = CounterPos{};
     m_pos.advance(m_offset);

@@ -3,6 +3,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <memory>
 
 namespace rb200
 {
@@ -109,21 +110,75 @@ void build_poisson_table(double lambda, HostPoissonTable& t)
     build_cdf(p, t.size, t.cdf);
 }
 
+namespace
+{
+
+// A table as kernel parameters (each struct stays under the 32 KB parameter limit).
+struct PoissonEntriesUpload
+{
+    unsigned long long* thr;
+    uint32_t*           alias;
+    uint32_t            size;
+    unsigned long long  thr_v[kPoissonTableCap];
+    uint32_t            alias_v[kPoissonTableCap];
+};
+
+struct PoissonDoublesUpload
+{
+    double*  dst;
+    uint32_t size;
+    double   v[kPoissonTableCap];
+};
+
+__global__ void poisson_upload_entries(const __grid_constant__ PoissonEntriesUpload u)
+{
+    for(uint32_t i = threadIdx.x; i < u.size; i += blockDim.x)
+    {
+        u.thr[i]   = u.thr_v[i];
+        u.alias[i] = u.alias_v[i];
+    }
+}
+
+__global__ void poisson_upload_doubles(const __grid_constant__ PoissonDoublesUpload u)
+{
+    for(uint32_t i = threadIdx.x; i < u.size; i += blockDim.x)
+        u.dst[i] = u.v[i];
+}
+
+rocrand_status upload_doubles(double* dst, const std::vector<double>& v, uint32_t size, cudaStream_t stream)
+{
+    auto u  = std::make_unique<PoissonDoublesUpload>();
+    u->dst  = dst;
+    u->size = size;
+    std::memcpy(u->v, v.data(), size * sizeof(double));
+    poisson_upload_doubles<<<1, 256, 0, stream>>>(*u);
+    return cudaGetLastError() == cudaSuccess ? ROCRAND_STATUS_SUCCESS : ROCRAND_STATUS_LAUNCH_FAILURE;
+}
+
+} // namespace
+
 PoissonCache::~PoissonCache()
 {
-    if(m_upload)
+    cudaFree(d_base);
+}
+
+rocrand_status PoissonCache::reserve()
+{
+    if(d_base != nullptr)
+        return ROCRAND_STATUS_SUCCESS;
+    static_assert(sizeof(PoissonEntriesUpload) < 32764 && sizeof(PoissonDoublesUpload) < 32764,
+                  "kernel parameters are limited to 32764 bytes");
+    const size_t cap = kPoissonTableCap;
+    if(cudaMalloc(&d_base, cap * (3 * sizeof(double) + sizeof(uint32_t))) != cudaSuccess)
     {
-        cudaEventSynchronize(m_upload);
-        cudaEventDestroy(m_upload);
+        d_base = nullptr;
+        return ROCRAND_STATUS_ALLOCATION_FAILED;
     }
-    cudaFree(d_prob);
-    cudaFree(d_thr);
-    cudaFree(d_alias);
-    cudaFree(d_cdf);
-    cudaFreeHost(h_prob);
-    cudaFreeHost(h_thr);
-    cudaFreeHost(h_alias);
-    cudaFreeHost(h_cdf);
+    d_thr   = reinterpret_cast<unsigned long long*>(d_base);
+    d_prob  = reinterpret_cast<double*>(d_base + cap * sizeof(double));
+    d_cdf   = reinterpret_cast<double*>(d_base + 2 * cap * sizeof(double));
+    d_alias = reinterpret_cast<uint32_t*>(d_base + 3 * cap * sizeof(double));
+    return ROCRAND_STATUS_SUCCESS;
 }
 
 rocrand_status PoissonCache::get(double lambda, cudaStream_t stream, bool with_cdf, DistParams& p)
@@ -135,50 +190,32 @@ rocrand_status PoissonCache::get(double lambda, cudaStream_t stream, bool with_c
         p.sqrt_lambda = std::sqrt(lambda);
         return ROCRAND_STATUS_SUCCESS;
     }
-    if(m_cap == 0)
-    {
-        m_cap = poisson_capacity(kPoissonHugeLambda);
-        if(cudaMalloc(&d_prob, m_cap * sizeof(double)) != cudaSuccess
-           || cudaMalloc(&d_thr, m_cap * sizeof(unsigned long long)) != cudaSuccess
-           || cudaMalloc(&d_alias, m_cap * sizeof(uint32_t)) != cudaSuccess
-           || cudaMalloc(&d_cdf, m_cap * sizeof(double)) != cudaSuccess
-           || cudaMallocHost(&h_prob, m_cap * sizeof(double)) != cudaSuccess
-           || cudaMallocHost(&h_thr, m_cap * sizeof(unsigned long long)) != cudaSuccess
-           || cudaMallocHost(&h_alias, m_cap * sizeof(uint32_t)) != cudaSuccess
-           || cudaMallocHost(&h_cdf, m_cap * sizeof(double)) != cudaSuccess
-           || cudaEventCreateWithFlags(&m_upload, cudaEventDisableTiming) != cudaSuccess)
-        {
-            m_cap = 0;
-            return ROCRAND_STATUS_ALLOCATION_FAILED;
-        }
-    }
+    rocrand_status st = reserve();
+    if(st != ROCRAND_STATUS_SUCCESS)
+        return st;
     if(lambda != m_lambda || (with_cdf && !m_has_cdf))
     {
         HostPoissonTable t;
         build_poisson_table(lambda, t);
-        // The staging buffers may still feed the previous upload.
-        if(m_pending && cudaEventSynchronize(m_upload) != cudaSuccess)
+        if(t.size > kPoissonTableCap)
             return ROCRAND_STATUS_INTERNAL_ERROR;
-        std::memcpy(h_prob, t.prob.data(), t.size * sizeof(double));
+        auto u   = std::make_unique<PoissonEntriesUpload>();
+        u->thr   = d_thr;
+        u->alias = d_alias;
+        u->size  = t.size;
         for(uint32_t i = 0; i < t.size; i++)
-            h_thr[i] = alias_entry(t.prob[i], t.alias[i]);
-        std::memcpy(h_alias, t.alias.data(), t.size * sizeof(uint32_t));
-        std::memcpy(h_cdf, t.cdf.data(), t.size * sizeof(double));
-        if(cudaMemcpyAsync(d_prob, h_prob, t.size * sizeof(double), cudaMemcpyHostToDevice, stream)
-               != cudaSuccess
-           || cudaMemcpyAsync(d_thr, h_thr, t.size * sizeof(unsigned long long), cudaMemcpyHostToDevice,
-                              stream)
-                  != cudaSuccess
-           || cudaMemcpyAsync(d_alias, h_alias, t.size * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                              stream)
-                  != cudaSuccess
-           || cudaMemcpyAsync(d_cdf, h_cdf, t.size * sizeof(double), cudaMemcpyHostToDevice, stream)
-                  != cudaSuccess
-           || cudaEventRecord(m_upload, stream) != cudaSuccess)
-            return ROCRAND_STATUS_INTERNAL_ERROR;
-        m_pending = true;
+            u->thr_v[i] = alias_entry(t.prob[i], t.alias[i]);
+        std::memcpy(u->alias_v, t.alias.data(), t.size * sizeof(uint32_t));
+        poisson_upload_entries<<<1, 256, 0, stream>>>(*u);
+        if(cudaGetLastError() != cudaSuccess)
+            return ROCRAND_STATUS_LAUNCH_FAILURE;
+        st = upload_doubles(d_prob, t.prob, t.size, stream);
+        if(st == ROCRAND_STATUS_SUCCESS && with_cdf)
+            st = upload_doubles(d_cdf, t.cdf, t.size, stream);
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
         m_lambda  = lambda;
-        m_has_cdf = true;
+        m_has_cdf = with_cdf;
         m_size    = t.size;
         m_offset  = t.offset;
     }

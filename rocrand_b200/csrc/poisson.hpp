@@ -4,7 +4,10 @@
 // operation order as the reference (library/src/rng/distribution/poisson.hpp:110-161 and
 // discrete.hpp:189-265), because Poisson output must be bit-exact and depends on
 // exp/lgamma of the host libm.  The device copy is refreshed in stream order when lambda
-// changes, like poisson_distribution_manager::get_distribution (poisson.hpp:277-351).
+// changes, like poisson_distribution_manager::get_distribution (poisson.hpp:277-351): the
+// new table travels as the parameters of a small upload kernel, so a call captured into a
+// CUDA graph carries its own table, and the update needs no host memory that must outlive
+// the call and no wait on earlier uploads.
 #pragma once
 
 #include "common.hpp"
@@ -58,6 +61,9 @@ inline unsigned long long alias_entry(double prob, uint32_t alias)
     return alias_threshold(prob) | (static_cast<unsigned long long>(alias) << 33);
 }
 
+// Largest table: poisson_capacity(kPoissonHugeLambda) = 2 * floor(16 * (2 + sqrt(4000))).
+constexpr uint32_t kPoissonTableCap = 2086;
+
 // Per-generator device cache of the table for the most recent lambda.
 class PoissonCache
 {
@@ -67,25 +73,24 @@ public:
     PoissonCache(const PoissonCache&)            = delete;
     PoissonCache& operator=(const PoissonCache&) = delete;
 
+    // Allocates the device tables (once; generators call it from init(), as the reference's
+    // generators initialise their Poisson manager, so that no allocation is left for a
+    // generate call that a stream capture records).
+    rocrand_status reserve();
+
     // Fills p with the distribution for lambda, uploading a new table on `stream` when
     // lambda changed.  with_cdf also uploads the cumulative table (used by Sobol).
     rocrand_status get(double lambda, cudaStream_t stream, bool with_cdf, DistParams& p);
 
 private:
-    double       m_lambda  = 0.0;
-    bool         m_has_cdf = false;
-    uint32_t     m_cap     = 0;
-    uint32_t     m_size = 0, m_offset = 0;
-    double*      d_prob  = nullptr;
-    unsigned long long* d_thr = nullptr; // packed alias entries (alias_entry)
-    uint32_t*    d_alias = nullptr;
-    double*      d_cdf   = nullptr;
-    double*      h_prob  = nullptr; // pinned staging
-    unsigned long long* h_thr = nullptr;
-    uint32_t*    h_alias = nullptr;
-    double*      h_cdf   = nullptr;
-    cudaEvent_t  m_upload = nullptr;
-    bool         m_pending = false;
+    double              m_lambda  = 0.0;
+    bool                m_has_cdf = false;
+    uint32_t            m_size = 0, m_offset = 0;
+    unsigned char*      d_base  = nullptr; // one allocation for the four tables
+    unsigned long long* d_thr   = nullptr; // packed alias entries (alias_entry)
+    double*             d_prob  = nullptr;
+    double*             d_cdf   = nullptr;
+    uint32_t*           d_alias = nullptr;
 };
 
 } // namespace rb200

@@ -144,6 +144,11 @@ public:
     {
         if(!m_initialized)
         {
+            // the Poisson tables are allocated here, as the reference's generators do in init(), so
+            // that a generate call recorded by a stream capture allocates nothing
+            const rocrand_status st = m_poisson.reserve();
+            if(st != ROCRAND_STATUS_SUCCESS)
+                return st;
             m_current     = static_cast<uint32_t>(m_offset); // 32-bit counter (sobol.hpp:604)
             m_initialized = true;
         }

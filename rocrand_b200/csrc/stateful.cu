@@ -587,6 +587,10 @@ public:
     {
         if(m_initialized)
             return ROCRAND_STATUS_SUCCESS;
+        // the Poisson tables are allocated here, as the reference's generators do in init(), so
+        // that a generate call recorded by a stream capture allocates nothing
+        if(m_poisson.reserve() != ROCRAND_STATUS_SUCCESS)
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
         if(m_arena == nullptr)
         {
             if(cudaMalloc(&m_arena, sizeof(uint32_t) * 6 * kE) != cudaSuccess)

@@ -322,6 +322,10 @@ public:
     {
         if(m_initialized)
             return ROCRAND_STATUS_SUCCESS;
+        // the Poisson tables are allocated here, as the reference's generators do in init(), so
+        // that a generate call recorded by a stream capture allocates nothing
+        if(m_poisson.reserve() != ROCRAND_STATUS_SUCCESS)
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
         // seed(seed, 0, offset): key from the seed (rocrand_threefry{2,4}x{32,64}_20.h seed())
         if constexpr(D == 4)
         {

@@ -77,11 +77,16 @@ def test_host_side_semantics(lib, rng):
         # pseudo generators have no dimensions and no uint4 seed
         assert lib.rocrand_set_quasi_random_generator_dimensions(g, 4) == rb.ROCRAND_STATUS_TYPE_ERROR
         assert lib.rocrand_set_seed_uint4(g, rb._Uint4(1, 2, 3, 4)) == rb.ROCRAND_STATUS_TYPE_ERROR
-        # a NULL output pointer initialises and returns SUCCESS (philox4x32_10.hpp:323-326)
+        # a NULL output pointer initialises and returns SUCCESS (philox4x32_10.hpp:323-326);
+        # initialising allocates the Poisson tables on the device (philox4x32_10.hpp:298), so
+        # on a machine without one both calls report that allocation failing, as the
+        # reference's do
+        import torch
+        init = 0 if torch.cuda.is_available() else rb.ROCRAND_STATUS_ALLOCATION_FAILED
         assert lib.rocrand_set_seed(g, 5) == 0
         assert lib.rocrand_set_offset(g, 17) == 0
-        assert lib.rocrand_generate_uniform(g, None, 100) == 0
-        assert lib.rocrand_initialize_generator(g) == 0
+        assert lib.rocrand_generate_uniform(g, None, 100) == init
+        assert lib.rocrand_initialize_generator(g) == init
     finally:
         assert lib.rocrand_destroy_generator(g) == 0
 
