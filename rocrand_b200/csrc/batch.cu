@@ -444,10 +444,16 @@ static rocrand_status poisson_for(double lambda, bool cdf, cudaStream_t stream, 
     static std::mutex                                                   mu;
     static std::map<std::tuple<int, double, bool>, std::unique_ptr<PoissonCache>> cache;
     std::lock_guard<std::mutex> lock(mu);
-    auto& slot = cache[std::make_tuple(device_info().device, lambda, cdf)];
-    if(!slot)
+    auto&      slot  = cache[std::make_tuple(device_info().device, lambda, cdf)];
+    const bool fresh = !slot;
+    if(fresh)
         slot.reset(new PoissonCache());
-    return slot->get(lambda, stream, cdf, p);
+    rocrand_status st = slot->get(lambda, stream, cdf, p);
+    // batches on every stream read the table: a new one is uploaded before anyone uses it
+    // (once per lambda; plans and the server build descriptors outside any stream capture)
+    if(st == ROCRAND_STATUS_SUCCESS && fresh && !p.huge && cudaStreamSynchronize(stream) != cudaSuccess)
+        st = ROCRAND_STATUS_LAUNCH_FAILURE;
+    return st;
 }
 
 rocrand_status batch_set_dist(BatchReq& r, uint32_t dist, double p0, double p1, cudaStream_t stream)
