@@ -17,6 +17,7 @@
 #include "batch.hpp"
 #include "common.hpp"
 #include "generators.hpp"
+#include "pool_allocator.hpp"
 
 #include <rocrand_b200.h>
 
@@ -44,59 +45,6 @@ double now_s()
     using namespace std::chrono;
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
-
-// First-fit allocator over the output pool (offsets, 512-byte granules).
-class PoolAllocator
-{
-public:
-    void reset(size_t bytes)
-    {
-        m_free.clear();
-        m_free[0] = bytes;
-        m_used    = 0;
-    }
-    bool alloc(size_t bytes, size_t& off)
-    {
-        bytes = (bytes + 511) & ~size_t(511);
-        for(auto it = m_free.begin(); it != m_free.end(); ++it)
-        {
-            if(it->second < bytes)
-                continue;
-            off              = it->first;
-            const size_t rem = it->second - bytes;
-            m_free.erase(it);
-            if(rem)
-                m_free[off + bytes] = rem;
-            m_used += bytes;
-            return true;
-        }
-        return false;
-    }
-    void release(size_t off, size_t bytes)
-    {
-        bytes = (bytes + 511) & ~size_t(511);
-        m_used -= bytes;
-        auto next = m_free.lower_bound(off);
-        if(next != m_free.end() && off + bytes == next->first)
-        {
-            bytes += next->second;
-            next = m_free.erase(next);
-        }
-        if(next != m_free.begin())
-        {
-            auto prev = std::prev(next);
-            if(prev->first + prev->second == off)
-            {
-                prev->second += bytes;
-                return;
-            }
-        }
-        m_free[off] = bytes;
-    }
-private:
-    std::map<size_t, size_t> m_free;
-    size_t                   m_used = 0;
-};
 
 struct Handle;
 
@@ -231,8 +179,12 @@ public:
             return ROCRAND_STATUS_TYPE_ERROR;
         if(n == 0)
             return ROCRAND_STATUS_OUT_OF_RANGE;
+        if(n > m_budget / batch_elem_size(dist)) // also keeps n * element size from wrapping
+            return ROCRAND_STATUS_OUT_OF_RANGE;
         const size_t bytes = n * batch_elem_size(dist);
-        if(bytes > m_budget)
+        // the pool hands out whole granules: a request whose granules exceed the budget could
+        // never be admitted, and admission does not overtake
+        if(PoolAllocator::granules(bytes) > m_budget)
             return ROCRAND_STATUS_OUT_OF_RANGE;
         std::lock_guard<std::mutex> lock(m_mu);
         if(handle >= m_handles.size())

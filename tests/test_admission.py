@@ -1,4 +1,6 @@
-"""The serving loop's admission policy (rocrand_b200/csrc/admission.hpp) on the host.
+"""The serving loop's host-side policies, run on the host: admission
+(rocrand_b200/csrc/admission.hpp) and the output pool's allocator
+(rocrand_b200/csrc/pool_allocator.hpp).
 
 tests/admission_check.cpp drives random queues of requests on stateful and stateless
 handles through the policy, with random batch limits and output budgets, and compares every
@@ -24,3 +26,17 @@ def test_admission_matches_full_scan(tmp_path):
     out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.split()[0] == "ok" and int(out.stdout.split()[1]) >= 40000
+
+
+def test_pool_allocator_first_fit_and_coalescing(tmp_path):
+    """tests/pool_allocator_check.cpp: random allocations and releases on the serving pool's
+    allocator (rocrand_b200/csrc/pool_allocator.hpp) against the list of live ranges --
+    in bounds, no overlap, first fit, failure only when nothing fits, free list coalesced."""
+    if shutil.which("g++") is None:
+        pytest.skip("no host C++ compiler")
+    exe = str(tmp_path / "pool_allocator_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-Wall", "-Werror", os.path.join(HERE, "pool_allocator_check.cpp"),
+                    "-o", exe], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.split()[0] == "ok" and int(out.stdout.split()[1]) >= 100000
