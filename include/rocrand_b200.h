@@ -126,7 +126,9 @@ rocrand_status ROCRANDAPI rocrand_b200_server_add_generator(rocrand_b200_server 
                                                             unsigned long long  seed,
                                                             unsigned int*       handle);
 /* Queues n values of `distribution` (parameters as in rocrand_b200_request) from the
- * handle's generator; the output is allocated from the pool when the request is admitted. */
+ * handle's generator; the output is allocated from the pool when the request is admitted.
+ * ROCRAND_STATUS_OUT_OF_RANGE for n == 0 or an output larger than the budget (counted in
+ * the pool's 512-byte granules); ROCRAND_STATUS_NOT_CREATED for an unknown handle. */
 rocrand_status ROCRANDAPI rocrand_b200_server_submit(rocrand_b200_server       server,
                                                      unsigned int              handle,
                                                      rocrand_b200_distribution distribution,
