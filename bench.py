@@ -46,6 +46,25 @@ PORT_SEEDED = {407}  # host streams seeded by the C port (the reference's host s
 STATEFUL = {401, 402, 405, 406}
 TWO_WORD = {"uniform_double", "normal", "normal_double", "log_normal", "log_normal_double"}
 
+# DRAM traffic of a launch from one ncu capture of the kernel on a smaller case (summaries in
+# profiles/): the state it reads is a fixed amount per launch, and every output byte is
+# written once (at the capture's size part of the output was still in L2 when the kernel
+# ended and was written back after it), so a launch of B output bytes moves read + B.
+NCU_TRAFFIC = {
+    ("mt19937", "normal_double"): (20.66e6, "profiles/mt_fill_normal_double_n2p24.md"),
+    ("philox4x32_10", "uniform"): (0.01e6, "profiles/philox_fill_fast_uniform_n2p26.md"),
+    ("philox4x32_10", "normal_double"): (0.05e6, "profiles/philox_fill_fast_normal_double_n2p24.md"),
+    ("mtgp32", "uint"): (2.2e6, "profiles/mtgp_fill_uint_n2p24.md"),
+}
+
+
+def ncu_traffic(gname, dist, out_bytes):
+    """(DRAM bytes per launch, source) scaled from the capture, or (None, None)."""
+    read, source = NCU_TRAFFIC.get((gname, dist), (None, None))
+    if read is None:
+        return None, None
+    return int(read + out_bytes), "%s: state read %.2f MB per launch + the output written once" % (source, read / 1e6)
+
 
 def rank_stream(gtype, dist, rank, n):
     """(seed, offset or None) giving rank `rank` the outputs [rank*n, (rank+1)*n) of the
@@ -336,12 +355,15 @@ def run_ours(args):
             "frac": round(dom_gbs / peak, 4),
             "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs copy bandwidth)" % peak_kind
             if peak_kind == "measured" else "fallback 6650 GB/s",
-            "traffic": None,
+            "traffic": ncu_traffic(calls[dom][0], calls[dom][2], dom_bytes)[0],
+            "traffic_source": ncu_traffic(calls[dom][0], calls[dom][2], dom_bytes)[1],
             "algorithmic_bytes_per_launch": dom_bytes,
         },
         "philox_uniform_2p28": {"kernel": "philox4x32_10 uniform fp32 n=2^28",
                        "achieved_gbs": round(ns_gbs, 1) if ns_gbs else None,
-                       "frac_of_peak": round(ns_gbs / peak, 4) if ns_gbs else None},
+                       "frac_of_peak": round(ns_gbs / peak, 4) if ns_gbs else None,
+                       "traffic": ncu_traffic("philox4x32_10", "uniform", 4 * (1 << 28))[0],
+                       "traffic_source": ncu_traffic("philox4x32_10", "uniform", 4 * (1 << 28))[1]},
         "per_call_ms": {"%s %s%s" % (c[0], c[2], "" if c[3] is None else list(c[3])): round(mean_call[i], 4)
                         for i, c in enumerate(calls)},
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0,
