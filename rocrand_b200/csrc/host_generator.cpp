@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <memory>
 
 namespace rb200
@@ -44,7 +45,7 @@ public:
         if(data == nullptr || n == 0)
             return m_inner->generate(data, n, d, p);
         void*          dev = nullptr;
-        rocrand_status st  = stage(data, n * dist_elem_size(d), dev);
+        rocrand_status st  = stage(data, n, dist_elem_size(d), dev);
         if(st != ROCRAND_STATUS_SUCCESS)
             return st;
         st = m_inner->generate(dev, n, d, p);
@@ -56,7 +57,7 @@ public:
         if(data == nullptr || n == 0)
             return m_inner->generate_poisson(data, n, lambda);
         void*          dev = nullptr;
-        rocrand_status st  = stage(data, n * sizeof(unsigned int), dev);
+        rocrand_status st  = stage(data, n, sizeof(unsigned int), dev);
         if(st != ROCRAND_STATUS_SUCCESS)
             return st;
         st = m_inner->generate_poisson(static_cast<unsigned int*>(dev), n, lambda);
@@ -64,10 +65,13 @@ public:
     }
 
 private:
-    // A device address congruent to `host` modulo 256 with `bytes` behind it.
-    rocrand_status stage(const void* host, size_t bytes, void*& dev)
+    // A device address congruent to `host` modulo 256 with n elements of `elem` bytes behind
+    // it (a count whose byte size would wrap cannot be a real host buffer: refused).
+    rocrand_status stage(const void* host, size_t n, size_t elem, void*& dev)
     {
-        const size_t need = bytes + 256;
+        if(n > (SIZE_MAX - 256) / elem)
+            return ROCRAND_STATUS_ALLOCATION_FAILED;
+        const size_t need = n * elem + 256;
         if(need > m_cap)
         {
             // the previous scratch may still be read by work queued on the stream
