@@ -706,6 +706,14 @@ rocrand_status BatchPlan::reserve(size_t reqs, size_t tiles)
         m_staged = nullptr;
         return ROCRAND_STATUS_INTERNAL_ERROR;
     }
+    // load the kernel and upload the per-device jump tables now (a module loads lazily at a
+    // kernel's first use, tens of ms, and the tables are copied on first use; both would
+    // otherwise land on the first batch)
+    cudaFuncAttributes attr;
+    if(cudaFuncGetAttributes(&attr, batch_fill) != cudaSuccess)
+        return ROCRAND_STATUS_LAUNCH_FAILURE;
+    if(stateful_xorwow_jump_polys() == nullptr || stateful_digit_tables(StatefulFamily::MRG32K3A) == nullptr)
+        return ROCRAND_STATUS_ALLOCATION_FAILED;
     return ROCRAND_STATUS_SUCCESS;
 }
 

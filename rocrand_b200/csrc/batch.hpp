@@ -102,7 +102,8 @@ public:
     // Serving batches (resident states, latency-bound mixes) take the serving tile sizes.
     void set_serving(bool serving) { m_serving = serving; }
     // Allocates the device tables and the pinned staging buffer for batches of up to `reqs`
-    // requests and `tiles` tiles now, so that the first batches do not allocate.
+    // requests and `tiles` tiles now, and loads the kernel, so that the first batches neither
+    // allocate nor wait for the module to load.
     rocrand_status reserve(size_t reqs, size_t tiles);
     // Assigns tiles and uploads the table on `stream`.
     rocrand_status upload(cudaStream_t stream);
