@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -841,14 +842,14 @@ rocrand_status BatchPlan::upload(cudaStream_t stream)
 
 static unsigned batch_grid()
 {
-    static int occ = 0;
+    static std::atomic<int> occ_cache{0}; // computed once; concurrent first calls agree
+    int                     occ = occ_cache.load(std::memory_order_relaxed);
     if(occ == 0)
     {
-        int b = 0;
-        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batch_fill, kBatchBlock, 0) != cudaSuccess
-           || b < 1)
-            b = 1;
-        occ = b;
+        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_fill, kBatchBlock, 0) != cudaSuccess
+           || occ < 1)
+            occ = 1;
+        occ_cache.store(occ, std::memory_order_relaxed);
     }
     const uint32_t per = batch_tuning().blocks_per_sm;
     const unsigned b   = per > 0 && per < static_cast<uint32_t>(occ) ? per : static_cast<unsigned>(occ);

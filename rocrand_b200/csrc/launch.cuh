@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 
 namespace rb200
@@ -34,17 +35,18 @@ __device__ __forceinline__ uint4 pack16(const T (&v)[N])
 template<class Kernel>
 inline unsigned grid_for(Kernel k, unsigned long long work, size_t smem)
 {
-    static int blocks_per_sm = 0;
-    if(blocks_per_sm == 0)
+    // threads launching the kernel for the first time may both compute it: same value
+    static std::atomic<int> blocks_per_sm{0};
+    int                     per = blocks_per_sm.load(std::memory_order_relaxed);
+    if(per == 0)
     {
-        int b = 0;
-        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kBlock, smem) != cudaSuccess
-           || b < 1)
-            b = 1;
-        blocks_per_sm = b;
+        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kBlock, smem) != cudaSuccess
+           || per < 1)
+            per = 1;
+        blocks_per_sm.store(per, std::memory_order_relaxed);
     }
     const unsigned long long full = static_cast<unsigned long long>(device_info().sm_count)
-                                    * static_cast<unsigned long long>(blocks_per_sm);
+                                    * static_cast<unsigned long long>(per);
     const unsigned long long need = (work + kBlock - 1) / kBlock;
     unsigned long long       g    = need < full ? need : full;
     return static_cast<unsigned>(g < 1 ? 1 : g);
