@@ -251,7 +251,10 @@ static const void* digit_tables(Family fam)
     if(cudaMemcpy(d, t32.empty() ? static_cast<const void*>(t64.data()) : t32.data(), bytes,
                   cudaMemcpyHostToDevice)
        != cudaSuccess)
+    {
+        cudaFree(d);
         return nullptr;
+    }
     c.ptr[dev] = d;
     return d;
 }
