@@ -161,3 +161,46 @@ def test_mt19937_host_side_semantics(lib):
         assert lib.rocrand_set_quasi_random_generator_dimensions(g, 2) == rb.ROCRAND_STATUS_TYPE_ERROR
     finally:
         assert lib.rocrand_destroy_generator(g) == 0
+
+
+C_CALLER = r"""
+#include <rocrand/rocrand.h>
+#include <rocrand_b200.h>
+#include <stdio.h>
+int main(void)
+{
+    rocrand_generator g;
+    int               v = 0;
+    if(rocrand_get_version(&v) != ROCRAND_STATUS_SUCCESS)
+        return 1;
+    if(rocrand_create_generator(&g, ROCRAND_RNG_QUASI_SOBOL32) != ROCRAND_STATUS_SUCCESS)
+        return 2;
+    if(rocrand_set_quasi_random_generator_dimensions(g, 64) != ROCRAND_STATUS_SUCCESS)
+        return 3;
+    if(rocrand_set_offset(g, 4096) != ROCRAND_STATUS_SUCCESS)
+        return 4;
+    if(rocrand_destroy_generator(g) != ROCRAND_STATUS_SUCCESS)
+        return 5;
+    printf("%d\n", v);
+    return 0;
+}
+"""
+
+
+def test_headers_compile_as_c_and_link(tmp_path, lib):
+    """A C caller (the reference's rocrand.h is a C header: rocrand.h:52-54) compiles with gcc
+    -std=c99 -Werror against include/, links against librocrand.so and runs its host calls."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "app.c"
+    src.write_text(C_CALLER)
+    exe = str(tmp_path / "app")
+    pkg = os.path.join(ROOT, "rocrand_b200")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    "-I", "/usr/local/cuda/include", "-o", exe, str(src), "-L", pkg, "-lrocrand",
+                    "-Wl,-rpath," + pkg], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, (out.returncode, out.stderr)
+    assert out.stdout.strip() == "300200"
