@@ -21,10 +21,13 @@ extern "C" {
  * `stream`, without allocating anything: for callers that cannot call cudaMalloc (inside a
  * CUDA graph capture or a driver callback, or with device memory fully pre-partitioned).
  * Its scratch (the alias table of lambda, up to 4096 entries) is a fixed 48 KiB array that
- * every GPU loading the library holds until the process exits; lambda <= 0 and tables
- * beyond 4096 entries give ROCRAND_STATUS_OUT_OF_RANGE.  The first call on a device looks
- * up the array's address and should come before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race.
+ * every GPU loading the library holds until the process exits; lambda <= 0, NaN and tables
+ * beyond 4096 entries give ROCRAND_STATUS_OUT_OF_RANGE.  The first call on a device, whatever
+ * its lambda, looks up the array's address and should come before any stream capture.  Each
+ * call writes its table into the array in stream order through a kernel's parameters, so a
+ * call recorded by a graph capture carries its own table.  All calls share the array: calls
+ * that overlap on the GPU race.  "Nothing" means device memory: no cudaMalloc or cudaFree is
+ * made; the host staging of the table is a per-thread block of the library.
  */
 rocrand_status ROCRANDAPI rocrand_b200_generate_poisson_noalloc(unsigned long long seed,
                                                                 unsigned long long offset,

@@ -268,7 +268,7 @@ rocrand_status ROCRANDAPI rocrand_generate_poisson(rocrand_generator generator,
 {
     if(generator == nullptr)
         return ROCRAND_STATUS_NOT_CREATED;
-    if(lambda <= 0.0)
+    if(!(lambda > 0.0)) // lambda <= 0 (and NaN)
         return ROCRAND_STATUS_OUT_OF_RANGE;
     return guarded([&] { return generator->generate_poisson(output_data, n, lambda); });
 }

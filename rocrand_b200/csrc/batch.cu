@@ -59,6 +59,7 @@ struct BatchLaunch
     const uint32_t*     xorwow_polys; // jump polynomials of the E engines
     const uint32_t*     xorwow_seqs;  // 2 x kXorwowSeqWords words per fresh XORWOW request
     const uint64_t*     mrg_tables;
+    lr::Table           logf; // host-logf replay table (Sobol normal)
 };
 
 // ---- distribution functors of each engine family, built from a descriptor ----
@@ -276,7 +277,7 @@ __device__ __forceinline__ void stateful_tile(const BatchReq& r, unsigned long l
 }
 
 template<SobolKind K>
-__device__ __forceinline__ void sobol_tile(const BatchReq& r, unsigned long long local)
+__device__ __forceinline__ void sobol_tile(const BatchReq& r, unsigned long long local, const lr::Table& logf)
 {
     using T                   = typename SobolOut<K, uint32_t>::T;
     constexpr unsigned PPT    = sizeof(T) >= 4 ? 4u : 16u / sizeof(T);
@@ -295,6 +296,7 @@ __device__ __forceinline__ void sobol_tile(const BatchReq& r, unsigned long long
     sp.offset      = r.toff;
     sp.lambda      = r.lambda;
     sp.sqrt_lambda = r.sqrt_lambda;
+    sp.logf        = logf;
     const uint32_t* v   = r.sobol_v;
     T*              row = reinterpret_cast<T*>(r.data);
     // the engine starts at the 32-bit sum offset + p (sobol.hpp:191-196)
@@ -390,15 +392,15 @@ __global__ void __launch_bounds__(kBatchBlock, 4) batch_fill(BatchLaunch L)
             default:
                 switch(r.dist)
                 {
-                    case BD_UINT: sobol_tile<SobolKind::UINT>(r, local); break;
-                    case BD_FLOAT: sobol_tile<SobolKind::FLOAT>(r, local); break;
-                    case BD_DOUBLE: sobol_tile<SobolKind::DOUBLE>(r, local); break;
-                    case BD_NORMAL_F: sobol_tile<SobolKind::NORMAL_F>(r, local); break;
+                    case BD_UINT: sobol_tile<SobolKind::UINT>(r, local, L.logf); break;
+                    case BD_FLOAT: sobol_tile<SobolKind::FLOAT>(r, local, L.logf); break;
+                    case BD_DOUBLE: sobol_tile<SobolKind::DOUBLE>(r, local, L.logf); break;
+                    case BD_NORMAL_F: sobol_tile<SobolKind::NORMAL_F>(r, local, L.logf); break;
                     default:
                         if(r.huge)
-                            sobol_tile<SobolKind::POISSON_HUGE>(r, local);
+                            sobol_tile<SobolKind::POISSON_HUGE>(r, local, L.logf);
                         else
-                            sobol_tile<SobolKind::POISSON>(r, local);
+                            sobol_tile<SobolKind::POISSON>(r, local, L.logf);
                         break;
                 }
                 break;
@@ -871,7 +873,7 @@ rocrand_status BatchPlan::launch(cudaStream_t stream)
     L.xorwow_polys  = stateful_xorwow_jump_polys();
     L.xorwow_seqs   = d_seq;
     L.mrg_tables    = static_cast<const uint64_t*>(stateful_digit_tables(StatefulFamily::MRG32K3A));
-    if(L.xorwow_polys == nullptr || L.mrg_tables == nullptr)
+    if(L.xorwow_polys == nullptr || L.mrg_tables == nullptr || !logf_replay_device(L.logf))
         return ROCRAND_STATUS_ALLOCATION_FAILED;
     const unsigned long long want = m_tiles;
     unsigned                 grid = batch_grid();
@@ -889,8 +891,9 @@ rocrand_status BatchPlan::replay(cudaStream_t stream)
     {
         // tables and the grid are resolved before capture (their first use uploads/queries)
         (void)batch_grid();
+        lr::Table lt;
         if(stateful_xorwow_jump_polys() == nullptr
-           || stateful_digit_tables(StatefulFamily::MRG32K3A) == nullptr)
+           || stateful_digit_tables(StatefulFamily::MRG32K3A) == nullptr || !logf_replay_device(lt))
             return ROCRAND_STATUS_ALLOCATION_FAILED;
         cudaStream_t cap = nullptr;
         if(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)

@@ -57,7 +57,7 @@ extern "C" {
 rocrand_status ROCRANDAPI rocrand_create_poisson_distribution(
     double lambda, rocrand_discrete_distribution* discrete_distribution)
 {
-    if(discrete_distribution == nullptr || lambda <= 0.0)
+    if(discrete_distribution == nullptr || !(lambda > 0.0)) // lambda <= 0 (and NaN)
         return ROCRAND_STATUS_OUT_OF_RANGE;
     try
     {

@@ -12,7 +12,10 @@
 //  * a table larger than that is rejected with ROCRAND_STATUS_OUT_OF_RANGE (Poisson
 //    tables for lambda <= 4000 have at most 2086 entries; larger lambdas need no table);
 //  * the device address of the array is looked up once per device, by the first call
-//    made on that device; make that first call before any stream capture;
+//    made on that device (whatever its lambda); make that first call before any stream
+//    capture;
+//  * each call writes its table into the array in stream order, through the parameters of
+//    a small kernel (no host memory has to outlive the call);
 //  * all calls share the array and each call rewrites the entries it uses, so calls that
 //    overlap on the GPU (different streams, no ordering between them) race.
 #include "common.hpp"
@@ -66,94 +69,29 @@ rocrand_status scratch_for_current_device(NoallocScratch& out)
     return ROCRAND_STATUS_SUCCESS;
 }
 
-// Host staging of one table, per calling thread (static storage: no heap allocation).
+// Host staging of one table, per calling thread: fixed-size arrays, so building a table
+// allocates nothing on the device and no heap memory.  (A thread's first call may make the
+// C library set up this thread-local block, as for any thread_local in a loaded library.)
 struct HostTable
 {
     double   p[kNoallocTableEntries];
     double   prob[kNoallocTableEntries];
-    unsigned long long thr[kNoallocTableEntries];
     uint32_t alias[kNoallocTableEntries];
     uint32_t small[kNoallocTableEntries];
     uint32_t large[kNoallocTableEntries];
 };
 thread_local HostTable t_table;
 
-// The Poisson alias table of lambda built exactly as the generator path builds it
-// (poisson.cpp, after library/src/rng/distribution/poisson.hpp:110-161 and
-// discrete.hpp:189-265), on fixed-size arrays.  Returns false when it does not fit.
+// The Poisson alias table of lambda, built by the generator path's own builder (poisson.cpp,
+// after library/src/rng/distribution/poisson.hpp:110-161 and discrete.hpp:189-265) on the
+// fixed-size arrays above.  Returns false when it does not fit.
 bool build_table(double lambda, uint32_t& size, uint32_t& offset)
 {
-    const size_t capacity = 2 * static_cast<size_t>(16.0 * (2.0 + std::sqrt(lambda)));
-    if(capacity > kNoallocTableEntries)
+    if(poisson_capacity(lambda) > kNoallocTableEntries)
         return false;
-    HostTable&   t          = t_table;
-    const double p_epsilon  = 1e-12;
-    const double log_lambda = std::log(lambda);
-    const int    left       = static_cast<int>(std::floor(lambda)) - static_cast<int>(capacity / 2);
-    std::memset(t.p, 0, sizeof(double) * capacity);
-    int lo = 0;
-    for(int i = static_cast<int>(capacity / 2); i >= 0; i--)
-    {
-        const double x  = left + i;
-        const double pp = std::exp(x * log_lambda - std::lgamma(x + 1.0) - lambda);
-        if(pp < p_epsilon)
-        {
-            lo = i + 1;
-            break;
-        }
-        t.p[i] = pp;
-    }
-    int hi = static_cast<int>(capacity) - 1;
-    for(int i = static_cast<int>(capacity / 2) + 1; i < static_cast<int>(capacity); i++)
-    {
-        const double x  = left + i;
-        const double pp = std::exp(x * log_lambda - std::lgamma(x + 1.0) - lambda);
-        if(pp < p_epsilon)
-        {
-            hi = i - 1;
-            break;
-        }
-        t.p[i] = pp;
-    }
-    for(int i = lo; i <= hi; i++)
-        t.p[i - lo] = t.p[i];
-    size   = static_cast<uint32_t>(hi - lo + 1);
-    offset = static_cast<uint32_t>(left + lo);
-    double sum = 0.0;
-    for(uint32_t i = 0; i < size; i++)
-        sum += t.p[i];
-    for(uint32_t i = 0; i < size; i++)
-        t.p[i] /= sum;
-
-    const double average = 1.0 / size;
-    uint32_t     ns = 0, nl = 0;
-    for(uint32_t i = 0; i < size; i++)
-    {
-        t.prob[i]  = 0.0;
-        t.alias[i] = 0;
-        if(t.p[i] >= average)
-            t.large[nl++] = i;
-        else
-            t.small[ns++] = i;
-    }
-    while(ns > 0 && nl > 0)
-    {
-        const uint32_t less = t.small[--ns];
-        const uint32_t more = t.large[--nl];
-        t.prob[less]        = t.p[less] * size;
-        t.alias[less]       = more;
-        t.p[more]           = (t.p[more] + t.p[less]) - average;
-        if(t.p[more] >= average)
-            t.large[nl++] = more;
-        else
-            t.small[ns++] = more;
-    }
-    for(uint32_t i = 0; i < ns; i++)
-        t.prob[t.small[i]] = 1.0;
-    for(uint32_t i = 0; i < nl; i++)
-        t.prob[t.large[i]] = 1.0;
-    for(uint32_t i = 0; i < size; i++)
-        t.thr[i] = alias_entry(t.prob[i], t.alias[i]);
+    HostTable& t = t_table;
+    poisson_probabilities_into(lambda, t.p, size, offset);
+    build_alias_into(t.p, size, t.prob, t.alias, t.small, t.large);
     return true;
 }
 
@@ -171,10 +109,16 @@ extern "C" rocrand_status ROCRANDAPI
                                           double             lambda,
                                           cudaStream_t       stream)
 {
-    if(lambda <= 0.0)
+    if(!(lambda > 0.0)) // also refuses NaN
         return ROCRAND_STATUS_OUT_OF_RANGE;
     try
     {
+        // Every call, whatever its lambda, first makes sure this device's scratch address
+        // is known, so that the first call on a device is the one that looks it up.
+        NoallocScratch s;
+        rocrand_status st = scratch_for_current_device(s);
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
         DistParams p;
         if(lambda > kPoissonHugeLambda)
         {
@@ -183,23 +127,16 @@ extern "C" rocrand_status ROCRANDAPI
             p.sqrt_lambda = std::sqrt(lambda);
             return philox_poisson_with_table(seed, offset, output_data, n, p, stream);
         }
-        NoallocScratch s;
-        rocrand_status st = scratch_for_current_device(s);
-        if(st != ROCRAND_STATUS_SUCCESS)
-            return st;
         uint32_t size = 0, table_offset = 0;
-        if(!build_table(lambda, size, table_offset))
+        if(!build_table(lambda, size, table_offset) || size > kPoissonTableCap)
             return ROCRAND_STATUS_OUT_OF_RANGE;
         if(output_data == nullptr || n == 0)
             return ROCRAND_STATUS_SUCCESS;
-        // Pageable sources: each copy returns once the source has been read, so the
-        // per-thread staging can be reused by the next call.
-        if(cudaMemcpyAsync(s.thr, t_table.thr, sizeof(unsigned long long) * size, cudaMemcpyHostToDevice, stream)
-               != cudaSuccess
-           || cudaMemcpyAsync(s.alias, t_table.alias, sizeof(uint32_t) * size,
-                              cudaMemcpyHostToDevice, stream)
-                  != cudaSuccess)
-            return ROCRAND_STATUS_INTERNAL_ERROR;
+        // The table travels as kernel parameters (stream-ordered; nothing on the host must
+        // outlive the call), as the generators' own tables do.
+        st = upload_alias_entries(s.thr, s.alias, t_table.prob, t_table.alias, size, stream);
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
         p.huge   = 0;
         p.thr    = s.thr;
         p.alias  = s.alias;

@@ -13,7 +13,7 @@ uint32_t poisson_capacity(double lambda)
     return static_cast<uint32_t>(2 * static_cast<size_t>(16.0 * (2.0 + std::sqrt(lambda))));
 }
 
-void poisson_probabilities(double lambda, std::vector<double>& p, uint32_t& size, uint32_t& offset)
+void poisson_probabilities_into(double lambda, double* p, uint32_t& size, uint32_t& offset)
 {
     // Probabilities are evaluated outwards from floor(lambda) and stop where they drop
     // below 1e-12, then shifted to start at index 0 (poisson.hpp:110-161).
@@ -21,7 +21,8 @@ void poisson_probabilities(double lambda, std::vector<double>& p, uint32_t& size
     const double p_epsilon  = 1e-12;
     const double log_lambda = std::log(lambda);
     const int    left       = static_cast<int>(std::floor(lambda)) - static_cast<int>(capacity / 2);
-    p.assign(capacity, 0.0);
+    for(size_t i = 0; i < capacity; i++)
+        p[i] = 0.0;
 
     int lo = 0;
     for(int i = static_cast<int>(capacity / 2); i >= 0; i--)
@@ -60,35 +61,54 @@ void poisson_probabilities(double lambda, std::vector<double>& p, uint32_t& size
         p[i] /= sum;
 }
 
-void build_alias(const std::vector<double>& p_in, uint32_t size, std::vector<double>& prob,
-                 std::vector<uint32_t>& alias)
+void poisson_probabilities(double lambda, std::vector<double>& p, uint32_t& size, uint32_t& offset)
+{
+    p.assign(poisson_capacity(lambda), 0.0);
+    poisson_probabilities_into(lambda, p.data(), size, offset);
+}
+
+void build_alias_into(double* p, uint32_t size, double* prob, uint32_t* alias, uint32_t* small,
+                      uint32_t* large)
 {
     // Vose's method with LIFO worklists; the pop order fixes which index becomes whose
     // alias, so it follows discrete.hpp:212-265 step for step.
-    std::vector<double> p(p_in.begin(), p_in.begin() + size);
+    const double average = 1.0 / size;
+    uint32_t     ns = 0, nl = 0;
+    for(uint32_t i = 0; i < size; i++)
+    {
+        prob[i]  = 0.0;
+        alias[i] = 0;
+        if(p[i] >= average)
+            large[nl++] = i;
+        else
+            small[ns++] = i;
+    }
+    while(ns > 0 && nl > 0)
+    {
+        const uint32_t less = small[--ns];
+        const uint32_t more = large[--nl];
+        prob[less]          = p[less] * size;
+        alias[less]         = more;
+        p[more]             = (p[more] + p[less]) - average;
+        if(p[more] >= average)
+            large[nl++] = more;
+        else
+            small[ns++] = more;
+    }
+    for(uint32_t i = 0; i < ns; i++)
+        prob[small[i]] = 1.0;
+    for(uint32_t i = 0; i < nl; i++)
+        prob[large[i]] = 1.0;
+}
+
+void build_alias(const std::vector<double>& p_in, uint32_t size, std::vector<double>& prob,
+                 std::vector<uint32_t>& alias)
+{
+    std::vector<double>   p(p_in.begin(), p_in.begin() + size);
+    std::vector<uint32_t> small(size), large(size);
     prob.assign(size, 0.0);
     alias.assign(size, 0u);
-    const double          average = 1.0 / size;
-    std::vector<uint32_t> small, large;
-    small.reserve(size);
-    large.reserve(size);
-    for(uint32_t i = 0; i < size; i++)
-        (p[i] >= average ? large : small).push_back(i);
-    while(!small.empty() && !large.empty())
-    {
-        const uint32_t less = small.back();
-        small.pop_back();
-        const uint32_t more = large.back();
-        large.pop_back();
-        prob[less]  = p[less] * size;
-        alias[less] = more;
-        p[more]     = (p[more] + p[less]) - average;
-        (p[more] >= average ? large : small).push_back(more);
-    }
-    for(uint32_t i : small)
-        prob[i] = 1.0;
-    for(uint32_t i : large)
-        prob[i] = 1.0;
+    build_alias_into(p.data(), size, prob.data(), alias.data(), small.data(), large.data());
 }
 
 void build_cdf(const std::vector<double>& p, uint32_t size, std::vector<double>& cdf)
@@ -145,6 +165,9 @@ __global__ void poisson_upload_doubles(const __grid_constant__ PoissonDoublesUpl
         u.dst[i] = u.v[i];
 }
 
+// Host staging of the entries upload, one per calling thread (the kernel launch copies it).
+thread_local PoissonEntriesUpload t_entries;
+
 rocrand_status upload_doubles(double* dst, const std::vector<double>& v, uint32_t size, cudaStream_t stream)
 {
     auto u  = std::make_unique<PoissonDoublesUpload>();
@@ -156,6 +179,24 @@ rocrand_status upload_doubles(double* dst, const std::vector<double>& v, uint32_
 }
 
 } // namespace
+
+rocrand_status upload_alias_entries(unsigned long long* thr, uint32_t* alias_dst, const double* prob,
+                                    const uint32_t* alias, uint32_t size, cudaStream_t stream)
+{
+    if(size > kPoissonTableCap)
+        return ROCRAND_STATUS_INTERNAL_ERROR;
+    PoissonEntriesUpload& u = t_entries;
+    u.thr                   = thr;
+    u.alias                 = alias_dst;
+    u.size                  = size;
+    for(uint32_t i = 0; i < size; i++)
+    {
+        u.thr_v[i]   = alias_entry(prob[i], alias[i]);
+        u.alias_v[i] = alias[i];
+    }
+    poisson_upload_entries<<<1, 256, 0, stream>>>(u);
+    return cudaGetLastError() == cudaSuccess ? ROCRAND_STATUS_SUCCESS : ROCRAND_STATUS_LAUNCH_FAILURE;
+}
 
 PoissonCache::~PoissonCache()
 {
@@ -199,17 +240,9 @@ rocrand_status PoissonCache::get(double lambda, cudaStream_t stream, bool with_c
         build_poisson_table(lambda, t);
         if(t.size > kPoissonTableCap)
             return ROCRAND_STATUS_INTERNAL_ERROR;
-        auto u   = std::make_unique<PoissonEntriesUpload>();
-        u->thr   = d_thr;
-        u->alias = d_alias;
-        u->size  = t.size;
-        for(uint32_t i = 0; i < t.size; i++)
-            u->thr_v[i] = alias_entry(t.prob[i], t.alias[i]);
-        std::memcpy(u->alias_v, t.alias.data(), t.size * sizeof(uint32_t));
-        poisson_upload_entries<<<1, 256, 0, stream>>>(*u);
-        if(cudaGetLastError() != cudaSuccess)
-            return ROCRAND_STATUS_LAUNCH_FAILURE;
-        st = upload_doubles(d_prob, t.prob, t.size, stream);
+        st = upload_alias_entries(d_thr, d_alias, t.prob.data(), t.alias.data(), t.size, stream);
+        if(st == ROCRAND_STATUS_SUCCESS)
+            st = upload_doubles(d_prob, t.prob, t.size, stream);
         if(st == ROCRAND_STATUS_SUCCESS && with_cdf)
             st = upload_doubles(d_cdf, t.cdf, t.size, stream);
         if(st != ROCRAND_STATUS_SUCCESS)

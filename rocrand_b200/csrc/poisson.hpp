@@ -37,10 +37,16 @@ uint32_t poisson_capacity(double lambda);
 // normalize (poisson.hpp:110-161, discrete.hpp:189-205).
 void poisson_probabilities(double lambda, std::vector<double>& p, uint32_t& size,
                            uint32_t& offset);
+// The same on caller storage: p must hold poisson_capacity(lambda) doubles.
+void poisson_probabilities_into(double lambda, double* p, uint32_t& size, uint32_t& offset);
 
 // Alias table (Vose, same stack order) and cumulative table of normalised p[0..size).
 void build_alias(const std::vector<double>& p, uint32_t size, std::vector<double>& prob,
                  std::vector<uint32_t>& alias);
+// The same on caller storage, allocating nothing: p[0..size) is consumed (overwritten),
+// prob / alias receive the table, small / large are work lists of `size` entries each.
+void build_alias_into(double* p, uint32_t size, double* prob, uint32_t* alias, uint32_t* small,
+                      uint32_t* large);
 void build_cdf(const std::vector<double>& p, uint32_t size, std::vector<double>& cdf);
 
 // Builds the full table for lambda (prob, alias and cdf).
@@ -63,6 +69,14 @@ inline unsigned long long alias_entry(double prob, uint32_t alias)
 
 // Largest table: poisson_capacity(kPoissonHugeLambda) = 2 * floor(16 * (2 + sqrt(4000))).
 constexpr uint32_t kPoissonTableCap = 2086;
+
+// Writes packed entries (alias_entry of prob[i], alias[i]) to thr[0..size) and alias[i] to
+// alias_dst[0..size) on `stream`.  The values travel as the parameters of one small kernel,
+// so the update is stream-ordered, is recorded whole by a CUDA graph capture, and needs no
+// host memory that outlives the call; the host staging is per calling thread.  size must
+// not exceed kPoissonTableCap.
+rocrand_status upload_alias_entries(unsigned long long* thr, uint32_t* alias_dst, const double* prob,
+                                    const uint32_t* alias, uint32_t size, cudaStream_t stream);
 
 // Per-generator device cache of the table for the most recent lambda.
 class PoissonCache

@@ -149,6 +149,10 @@ public:
             const rocrand_status st = m_poisson.reserve();
             if(st != ROCRAND_STATUS_SUCCESS)
                 return st;
+            // likewise the device tables every generate call reads (uploaded once per device)
+            lr::Table lt;
+            if(sobol_device_vectors(kIs64, kScrambled) == nullptr || !logf_replay_device(lt))
+                return ROCRAND_STATUS_ALLOCATION_FAILED;
             m_current     = static_cast<uint32_t>(m_offset); // 32-bit counter (sobol.hpp:604)
             m_initialized = true;
         }
@@ -228,6 +232,10 @@ public:
         p.offset      = dp.offset;
         p.lambda      = dp.lambda;
         p.sqrt_lambda = dp.sqrt_lambda;
+        if((d == Dist::NORMAL_F32 || d == Dist::LOGNORMAL_F32 || d == Dist::NORMAL_F16
+            || d == Dist::LOGNORMAL_F16)
+           && !logf_replay_device(p.logf))
+            return ROCRAND_STATUS_INTERNAL_ERROR;
         switch(d)
         {
             case Dist::U32: st = launch<SobolKind::UINT>(data, n, p); break;

@@ -4,6 +4,7 @@
 
 #include "common.hpp"
 #include "dist.cuh"
+#include "logf_replay.cuh"
 
 namespace rb200
 {
@@ -11,12 +12,13 @@ namespace rb200
 // ---- distributions over a Sobol value (sobol_*_distribution, uniform.hpp:351-442,
 //      normal.hpp:272-330, log_normal.hpp:296-370, poisson.hpp CDF method) ----
 
-// rocrand_normal.h:174-194 roc_f_erfinv, every step rounded as written.
-__device__ __forceinline__ float erfinv_f(float x)
+// rocrand_normal.h:174-194 roc_f_erfinv, every step rounded as written; the logarithm is the
+// host C library's logf (logf_replay.cuh), which the outer cancellation amplifies.
+__device__ __forceinline__ float erfinv_f(float x, const lr::Table& logf_table)
 {
     const float sgn = (x < 0.0f) ? -1.0f : 1.0f;
     x               = __fmul_rn(__fsub_rn(1.0f, x), __fadd_rn(1.0f, x));
-    const float lnx = pm::logf(x);
+    const float lnx = lr::logf_host(x, logf_table);
     if(isnan(lnx))
         return 1.0f;
     if(isinf(lnx))
@@ -27,10 +29,10 @@ __device__ __forceinline__ float erfinv_f(float x)
 }
 
 // normal_distribution(unsigned int) (rocrand_normal.h:228-233); a 64-bit value uses its high word.
-__device__ __forceinline__ float sobol_normal_f(uint32_t hi32)
+__device__ __forceinline__ float sobol_normal_f(uint32_t hi32, const lr::Table& logf_table)
 {
     const float p = u32_to_f32(hi32);
-    return __fmul_rn(RB_SQRT2, erfinv_f(__fsub_rn(__fmul_rn(2.0f, p), 1.0f)));
+    return __fmul_rn(RB_SQRT2, erfinv_f(__fsub_rn(__fmul_rn(2.0f, p), 1.0f), logf_table));
 }
 
 template<class W>
@@ -100,6 +102,7 @@ struct SobolParams
     const double* cdf;
     uint32_t      size, offset;
     double        lambda, sqrt_lambda;
+    lr::Table     logf; // fp32 normal kinds: the host-logf replay table
 };
 
 template<SobolKind K, class W>
@@ -122,17 +125,17 @@ __device__ __forceinline__ typename SobolOut<K, W>::T sobol_apply(W x, const Sob
     else if constexpr(K == SobolKind::HALF)
         return u16_to_f16(static_cast<uint32_t>(x >> (B - 16)) & 0xffffu);
     else if constexpr(K == SobolKind::NORMAL_F)
-        return __fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x)), p.std_f));
+        return __fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x), p.logf), p.std_f));
     else if constexpr(K == SobolKind::LOGNORMAL_F)
-        return expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x)))));
+        return expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x), p.logf))));
     else if constexpr(K == SobolKind::NORMAL_D)
         return __dadd_rn(p.mean_d, __dmul_rn(sobol_normal_d(x), p.std_d));
     else if constexpr(K == SobolKind::LOGNORMAL_D)
         return exp(__dadd_rn(p.mean_d, __dmul_rn(p.std_d, sobol_normal_d(x))));
     else if constexpr(K == SobolKind::NORMAL_H)
-        return __float2half_rn(__fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x)), p.std_f)));
+        return __float2half_rn(__fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x), p.logf), p.std_f)));
     else if constexpr(K == SobolKind::LOGNORMAL_H)
-        return __float2half_rn(expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x))))));
+        return __float2half_rn(expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x), p.logf)))));
     else if constexpr(K == SobolKind::POISSON)
     {
         // discrete_cdf (rocrand_discrete.h:92-115): first entry >= x, capped at the last

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.hpp"
+#include "logf_replay.cuh"
 
 #include <vector>
 
@@ -24,5 +25,9 @@ const SobolTables& sobol_tables();
 
 // Device copy of one table on the current device (uploaded once per device).
 const void* sobol_device_vectors(bool is64, bool scrambled);
+
+// The host-logf replay table of the inverse-erf normal (logf_replay.cuh) on the current
+// device, uploaded once per device; false if it is missing or could not be uploaded.
+bool logf_replay_device(lr::Table& out);
 
 } // namespace rb200

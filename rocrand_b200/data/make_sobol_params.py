@@ -21,7 +21,7 @@ Output format (little-endian bit stream, LSB first): magic "RBSOBOL1", uint32 di
 m_j (j+1 bits each, j = 0..s-1).
 
 Usage (in a checkout that has the reference sources):
-    python rocrand_b200/data/make_sobol_params.py /root/reference/library/src/rocrand_sobol32_precomputed.bin
+    python rocrand_b200/data/make_sobol_params.py <reference>/library/src/rocrand_sobol32_precomputed.bin
 """
 
 import os

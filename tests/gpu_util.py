@@ -12,6 +12,19 @@ from oracle import pyorc
 BIT_EXACT = {"uint", "ulonglong", "char", "short", "uniform", "uniform_double", "uniform_half",
              "poisson"}
 
+# Sobol's fp32 normal (and its half form) is bit-exact too: its only transcendental, logf, is
+# the host C library's own result (logf_replay.cuh), and every other step is IEEE.
+SOBOL_EXACT = {"normal", "normal_half"}
+
+
+def bit_exact(rng, dist):
+    return dist in BIT_EXACT or (rng in SOBOL and dist in SOBOL_EXACT)
+
+
+# Elements of fp64 outputs that are outside the forward ulp bound and were accepted by the
+# backward-error rule of compare_call, per (rng, dist): [accepted elements, elements compared].
+FP64_EXCEPTIONS = {}
+
 # ulp tolerances of the floating-point distributions against the host oracle (glibc libm).
 # They bound the error of the deviate the library computes, stddev * N, in ulps of that
 # deviate: <= 4 ulp for fp32, <= 2 ulp for fp64, <= 1 ulp for half (rounded from fp32).
@@ -47,6 +60,13 @@ def device_generate(lib, g, dist, n, params=(), mis=0):
     st = fn(g, c_void_p(view.data_ptr()), c_size_t(n), *pyorc.dist_args(dist, params))
     torch.cuda.synchronize()
     return st, view.cpu().numpy().view(dt)
+
+
+def generate_into(lib, g, dist, buf, params=()):
+    """One generate call writing buf (a contiguous torch tensor on the device); the status."""
+    suffix = pyorc.DISTS[dist][0]
+    fn = getattr(lib, "rocrand_" + suffix)
+    return fn(g, c_void_p(buf.data_ptr()), c_size_t(buf.numel()), *pyorc.dist_args(dist, params))
 
 
 def create(lib, rng, seed=None, offset=None, dims=None):
@@ -111,6 +131,9 @@ def _ratios(dist, got, exp, params):
     return ratio
 
 
+SOBOL = {501, 502, 504, 505}
+
+
 def compare(dist, got, exp, params=(), alts=()):
     """Asserts parity of one output; returns the max ulp distance (0 for bit-exact).
     Elements outside the tolerance of `exp` may instead be within it of one of `alts`."""
@@ -136,7 +159,6 @@ def compare(dist, got, exp, params=(), alts=()):
     return worst_ulps
 
 
-SOBOL = {501, 502, 504, 505}
 
 
 def erfinv_normal(rng, dist):
@@ -148,27 +170,30 @@ def erfinv_normal(rng, dist):
 
 
 def libm_shifts(rng, dist):
-    """(log, sin/cos) ulp shifts of the host library's results under which a device output
-    may instead match the reference formula: the inverse-erf normal (log only) and the
-    fp64 Box-Muller transforms (log and sin/cos)."""
+    """(log, sin/cos) ulp shifts of the host library's fp64 results under which a device
+    output may instead match the reference formula: the fp64 inverse-erf normal (log only)
+    and the fp64 Box-Muller transforms (log and sin/cos).  fp32 outputs have none: they must
+    meet the forward bound (or be bit-exact)."""
+    if dist not in ("normal_double", "log_normal_double"):
+        return []
     if erfinv_normal(rng, dist):
         return [(1, 0), (-1, 0)]
-    if dist in ("normal_double", "log_normal_double"):
-        return [(a, b) for a in (-1, 0, 1) for b in (-1, 0, 1) if (a, b) != (0, 0)]
-    return []
+    return [(a, b) for a in (-1, 0, 1) for b in (-1, 0, 1) if (a, b) != (0, 0)]
 
 
 def compare_call(orc, rng, seed, offset, dims, calls, k, got, exp):
-    """compare() for call k of a sequence, with a backward-error fallback on the host
-    library's transcendentals.  The oracle evaluates the reference's formulas with glibc's
-    log/sin/cos, which are themselves not correctly rounded in a fraction of a percent of
-    inputs; the device's are (precise_math.cuh).  Two places amplify a one-ulp difference
-    there beyond the ulp bound: the inverse-erf normal (sqrt(-tt1 + sqrt(tt1^2 - tt2)) with
-    tt1, tt2 linear in log(x) cancels, tens of ulps), and the fp64 Box-Muller products (one
-    ulp of sin can be two of the output).  An element outside the ulp tolerance must then
-    be within it of the reference formula evaluated with glibc's results moved by one ulp
-    (the oracle rerun with those values); every other operation is IEEE and identical."""
+    """Parity of call k of a sequence.  Bit-exact classes must be identical; fp32 and half
+    normals and log-normals must meet the forward ulp bound.  fp64 normals and log-normals
+    must meet it too, except for elements where the host library's own log/sin/cos result is
+    not correctly rounded and the reference formula amplifies that: the fp64 inverse-erf
+    normal (sqrt(-tt1 + sqrt(tt1^2 - tt2)), tt1 and tt2 linear in log(x), cancels: tens of
+    ulps) and the fp64 Box-Muller products (one ulp of sin can be two of the output).  Such
+    an element is accepted only if it is within the bound of the reference formula evaluated
+    with glibc's results moved by one ulp (the oracle rerun with those values; every other
+    operation is IEEE and identical), and it is counted in FP64_EXCEPTIONS."""
     dist, _, params, _ = calls[k]
+    if bit_exact(rng, dist):
+        return compare("uint" if dist not in BIT_EXACT else dist, got, exp, params)
     try:
         return compare(dist, got, exp, params)
     except AssertionError:
@@ -182,4 +207,9 @@ def compare_call(orc, rng, seed, offset, dims, calls, k, got, exp):
             alts.append(pyorc.run_sequence(orc, rng, seed, offset, calls[:k + 1], dims=dims)[k][1])
         finally:
             orc.set_libm_ulps(0, 0)
-    return compare(dist, got, exp, params, alts)
+    worst = compare(dist, got, exp, params, alts)
+    outside = int((_ratios(dist, got, exp, params) > 1.0).sum())
+    acc = FP64_EXCEPTIONS.setdefault((rng, dist), [0, 0])
+    acc[0] += outside
+    acc[1] += int(exp.size)
+    return worst

@@ -51,7 +51,7 @@ def test_golden_replay(lib, orc, name):
                 assert st == exp["status"] == ost
                 if st != 0:
                     continue
-                if dist in gu.BIT_EXACT:
+                if gu.bit_exact(case["rng"], dist):
                     assert gu.sha(vals) == exp["sha256"], (name, dist, n, mis)
                 gu.compare_call(orc, case["rng"], case.get("seed"), case.get("offset"), case.get("dims"),
                                 calls, k, vals, ovals)
@@ -127,46 +127,121 @@ def test_mt19937_mixed_sequences(lib, orc, seed):
         lib.rocrand_destroy_generator(g)
 
 
+def _full_digests():
+    with open(os.path.join(HERE, "golden", "full_digests.json")) as f:
+        return json.load(f)
+
+
+def _device_call(lib, rng, seed, offset, dims, dist, n, params):
+    """One generate call of n values on a fresh generator; the torch tensor on the device."""
+    import torch
+    g = gu.create(lib, rng, seed, offset, dims)
+    try:
+        buf = torch.empty(n, dtype=gu.torch_dtype(dist), device="cuda")
+        st = gu.generate_into(lib, g, dist, buf, params)
+        assert st == 0, st
+        torch.cuda.synchronize()
+    finally:
+        lib.rocrand_destroy_generator(g)
+    return buf
+
+
+def _continuity(lib, name, dist, params, big):
+    """The same stream produced by 3 calls of the same total is identical (compared on the
+    device)."""
+    import torch
+    n = big.numel()
+    offset = None if name in NO_OFFSET else 0
+    g = gu.create(lib, PSEUDO[name], 0xdeadbeef, offset)
+    parts = [(1 << 27) + 12, (1 << 26) - 4, n - (1 << 27) - (1 << 26) - 8]
+    cat = torch.empty_like(big)
+    pos = 0
+    try:
+        for k in parts:
+            assert gu.generate_into(lib, g, dist, cat[pos:pos + k], params) == 0
+            pos += k
+        torch.cuda.synchronize()
+    finally:
+        lib.rocrand_destroy_generator(g)
+    return cat, parts
+
+
+@pytest.mark.parametrize("name", sorted(PSEUDO))
+@pytest.mark.parametrize("dist", ["uniform", "uint"])
+def test_full_size_digest_and_continuity(lib, orc, name, dist):
+    """2^28 values in one call hash to the digest recorded from the reference's own host
+    generator (tests/golden/make_full_digests.py), and the same stream made by 3 calls of the
+    same total is identical (MTGP32, whose stream depends on the split, is compared with the
+    oracle making the same 3 calls)."""
+    import torch
+    n = 1 << 28
+    ent = _full_digests()["%s/%s/2^28" % (name, dist)]
+    assert ent["call"][1] == n and ent["seed"] == 0xdeadbeef
+    offset = None if name in NO_OFFSET else 0
+    big = _device_call(lib, PSEUDO[name], 0xdeadbeef, offset, None, dist, n, [])
+    assert gu.sha(big.cpu().numpy()) == ent["sha256"], (name, dist)
+    if dist != "uniform":
+        return
+    cat, parts = _continuity(lib, name, dist, [], big)
+    if name in SPLIT_DIFFERS:
+        seq = [(dist, k, [], 0) for k in parts]
+        ref = pyorc.run_sequence(orc, PSEUDO[name], 0xdeadbeef, offset, seq)
+        pos = 0
+        for k, (ost, ovals) in zip(parts, ref):
+            assert ost == 0
+            gu.compare(dist, cat[pos:pos + k].cpu().numpy(), ovals)
+            pos += k
+    else:
+        assert torch.equal(cat, big)
+    del big, cat
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("name", sorted(PSEUDO))
+def test_full_size_normal(lib, orc, name):
+    """Normal fp32 at 2^28 in one call: the first 2^22 values equal the oracle's (the
+    oracle's first 2^22 values are those of a call of that size), and the same stream made
+    by 3 calls of the same total is identical (MTGP32: its first call against the oracle's
+    same call).  The comparison of all 2^28 values with the oracle is the slow test below."""
+    import torch
+    n, head = 1 << 28, 1 << 22
+    params = [0.0, 1.0]
+    offset = None if name in NO_OFFSET else 0
+    big = _device_call(lib, PSEUDO[name], 0xdeadbeef, offset, None, "normal", n, params)
+    ost, ovals = pyorc.run_sequence(orc, PSEUDO[name], 0xdeadbeef, offset, [("normal", head, params, 0)])[0]
+    assert ost == 0
+    gu.compare_call(orc, PSEUDO[name], 0xdeadbeef, offset, None, [("normal", head, params, 0)], 0,
+                    big[:head].cpu().numpy(), ovals)
+    cat, parts = _continuity(lib, name, "normal", params, big)
+    if name in SPLIT_DIFFERS:
+        ost, ovals = pyorc.run_sequence(orc, PSEUDO[name], 0xdeadbeef, offset,
+                                        [("normal", head + 12, params, 0)])[0]
+        g = gu.create(lib, PSEUDO[name], 0xdeadbeef, offset)
+        try:
+            st, first = gu.device_generate(lib, g, "normal", head + 12, params, 0)
+        finally:
+            lib.rocrand_destroy_generator(g)
+        assert st == ost == 0
+        gu.compare("normal", first, ovals, params)
+    else:
+        assert torch.equal(cat, big)
+    del big, cat
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.slow
 @pytest.mark.parametrize("name", sorted(PSEUDO))
 @pytest.mark.parametrize("dist", ["uniform", "normal"])
-def test_full_size_against_oracle_and_continuity(lib, orc, name, dist):
-    """2^28 values in one call equal the oracle's 2^28 values, and the same stream produced
-    by 3 calls of the same total is identical."""
-    import torch
+def test_full_size_against_oracle(lib, orc, name, dist):
+    """All 2^28 values of one call against the oracle's (slow: the oracle runs on one host
+    core; run with --runslow)."""
     n = 1 << 28
     params = [0.0, 1.0] if dist == "normal" else []
     offset = None if name in NO_OFFSET else 0
-    g = gu.create(lib, PSEUDO[name], 0xdeadbeef, offset)
-    st, big = gu.device_generate(lib, g, dist, n, params, 0)
-    assert st == 0
-    lib.rocrand_destroy_generator(g)
+    big = _device_call(lib, PSEUDO[name], 0xdeadbeef, offset, None, dist, n, params).cpu().numpy()
     ost, ovals = pyorc.run_sequence(orc, PSEUDO[name], 0xdeadbeef, offset, [(dist, n, params, 0)])[0]
     assert ost == 0
     gu.compare_call(orc, PSEUDO[name], 0xdeadbeef, offset, None, [(dist, n, params, 0)], 0, big, ovals)
-    del ovals
-    # continuity: 3 calls of the same total
-    g = gu.create(lib, PSEUDO[name], 0xdeadbeef, offset)
-    parts = [(1 << 27) + 12, (1 << 26) - 4, n - (1 << 27) - (1 << 26) - 8]
-    got = []
-    for k in parts:
-        st, v = gu.device_generate(lib, g, dist, k, params, 0)
-        assert st == 0
-        got.append(v)
-    lib.rocrand_destroy_generator(g)
-    if name in SPLIT_DIFFERS:
-        # a call ends the partial round of every block generator (mtgp32.hpp:268-305): the
-        # stream depends on how it is split, so the 3 calls are checked against the oracle
-        del big
-        seq = [(dist, k, params, 0) for k in parts]
-        ref = pyorc.run_sequence(orc, PSEUDO[name], 0xdeadbeef, offset, seq)
-        for i, (v, (ost, ovals)) in enumerate(zip(got, ref)):
-            assert ost == 0
-            gu.compare_call(orc, PSEUDO[name], 0xdeadbeef, offset, None, seq, i, v, ovals)
-        return
-    cat = np.concatenate(got)
-    assert np.array_equal(cat.view(np.uint8), big.view(np.uint8))
-    del big, cat, got
-    torch.cuda.empty_cache()
 
 
 @pytest.mark.parametrize("name", sorted(QUASI))
@@ -199,18 +274,17 @@ def test_quasi_random_sequences(lib, orc, name, dist, params):
                                        ("scrambled_sobol64", 1), ("scrambled_sobol64", 64),
                                        ("scrambled_sobol64", 1000)])
 @pytest.mark.parametrize("dist", ["uniform_double", "normal"])
-def test_quasi_config_sizes(lib, orc, name, dims, dist):
-    """The quasi-random workload: 2^20 points per dimension at offset 4096, dimension-major,
-    compared with the oracle in full."""
+def test_quasi_config_sizes(lib, name, dims, dist):
+    """The quasi-random workload: 2^20 points per dimension at offset 4096, dimension-major.
+    Both outputs are bit-exact (uniform fp64 by construction, the fp32 normal through the
+    host-logf replay), so the whole output must hash to the digest recorded from the
+    reference's own host generator (tests/golden/make_full_digests.py)."""
     import torch
     n = dims << 20
+    ent = _full_digests()["%s/%s/dims%d" % (name, dist, dims)]
+    assert ent["call"][1] == n and ent["offset"] == 4096 and ent["dims"] == dims
     params = [0.0, 1.0] if dist == "normal" else []
-    g = gu.create(lib, QUASI[name], None, 4096, dims)
-    st, vals = gu.device_generate(lib, g, dist, n, params, 0)
-    lib.rocrand_destroy_generator(g)
-    assert st == 0
-    ost, ovals = pyorc.run_sequence(orc, QUASI[name], None, 4096, [(dist, n, params, 0)], dims=dims)[0]
-    assert ost == 0
-    gu.compare_call(orc, QUASI[name], None, 4096, dims, [(dist, n, params, 0)], 0, vals, ovals)
-    del vals, ovals
+    vals = _device_call(lib, QUASI[name], None, 4096, dims, dist, n, params)
+    assert gu.sha(vals.cpu().numpy()) == ent["sha256"], (name, dist, dims)
+    del vals
     torch.cuda.empty_cache()

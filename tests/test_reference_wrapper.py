@@ -17,7 +17,7 @@ import sys
 
 import pytest
 
-REFERENCE = "/root/reference"
+REFERENCE = os.environ.get("ROCRAND_REFERENCE", "/root/reference")
 BINDING = os.path.join(REFERENCE, "python", "rocrand")
 SUITE = os.path.join(BINDING, "tests", "rocrand_test.py")
 PACKAGE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "rocrand_b200")
