@@ -40,7 +40,13 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Generator families in the sweep (rocrand_rng_type values), in the order they were built.
 SWEEP_GENERATORS = [("philox4x32_10", 404), ("xorwow", 401), ("mrg32k3a", 402), ("lfsr113", 406),
-                    ("mt19937", 407), ("threefry4x32_20", 410), ("mtgp32", 403)]
+                    ("mt19937", 407), ("threefry4x32_20", 410), ("mtgp32", 403), ("mrg31k3p", 405),
+                    ("threefry2x32_20", 408), ("threefry2x64_20", 409), ("threefry4x64_20", 411)]
+# The quasi-random workload: Sobol32 and scrambled Sobol64, 1 / 64 / 1000 dimensions x 2^20
+# points at offset 4096, uniform fp64 and normal fp32 (dimension-major output).
+QUASI_GENERATORS = [("sobol32", 501), ("scrambled_sobol64", 505)]
+QUASI_DIMS = [1, 64, 1000]
+QUASI_DISTS = [("uniform_double", None), ("normal", (0.0, 1.0))]
 NO_OFFSET = {407, 403}  # MT19937, MTGP32: set_offset is a TYPE_ERROR
 PORT_SEEDED = {407}  # host streams seeded by the C port (the reference's host seeding is slow)
 STATEFUL = {401, 402, 405, 406}
@@ -56,6 +62,13 @@ NCU_TRAFFIC = {
     ("philox4x32_10", "normal_double"): (0.05e6, "profiles/philox_fill_fast_normal_double_n2p24.md"),
     ("mtgp32", "uint"): (2.2e6, "profiles/mtgp_fill_uint_n2p24.md"),
 }
+
+
+# Warp instructions per output value of each sweep kernel (sm__inst_executed.sum / n) from one
+# ncu capture of the sweep at n = 2^24 (profiles/sweep_instructions_n2p24.md); the issue bound
+# of a kernel is these instructions at 4 per SM per clock.  Filled from that capture.
+NCU_INST_SOURCE = "profiles/sweep_instructions_n2p24.md"
+NCU_INST = {}
 
 
 def ncu_traffic(gname, dist, out_bytes):
@@ -271,19 +284,31 @@ def run_ours(args):
     step_bytes = sum(ELEM[d] * n for _, _, d, _ in calls)
     value = step_bytes * world * args.steps / (total_ms * 1e-3) / 1e9
 
-    # dominant kernel: the call with the largest device time in the step
+    # per-kernel rooflines: achieved write GB/s against the smaller of the measured HBM peak
+    # and the kernel's issue bound (NCU_INST at the sampled clock); the dominant kernel is the
+    # call with the largest device time in the step
     mean_call = [statistics.mean(per_call_ms[s][i] for s in range(args.steps)) for i in range(len(calls))]
-    dom = max(range(len(calls)), key=lambda i: mean_call[i])
     peak, peak_kind = measured_peak()
-    dom_bytes = ELEM[calls[dom][2]] * n
-    dom_gbs = dom_bytes / (mean_call[dom] * 1e-3) / 1e9
-    # headline kernel: Philox uniform fp32 at 2^28
+
+    def kernel_roof(i):
+        gname, _, d, _ = calls[i]
+        b = ELEM[d] * n
+        gbs = b / (mean_call[i] * 1e-3) / 1e9
+        iss, iss_src = issue_bound(gname, d, n, clocks.get("sm_mhz"))
+        bound = "issue" if iss is not None and iss < peak else "hbm"
+        lim = min(peak, iss) if iss is not None else peak
+        return {"kernel": "%s %s%s" % (gname, d, "" if calls[i][3] is None else list(calls[i][3])),
+                "bytes": b, "gbs": gbs, "hbm_frac": gbs / peak,
+                "issue_gbs": iss, "issue_frac": (gbs / iss) if iss else None, "bound": bound,
+                "frac": gbs / lim, "issue_source": iss_src}
+
+    roofs = [kernel_roof(i) for i in range(len(calls))]
+    dom = max(range(len(calls)), key=lambda i: mean_call[i])
     ns = [i for i, c in enumerate(calls) if c[0] == "philox4x32_10" and c[2] == "uniform"]
-    ns_gbs = (4 * n) / (mean_call[ns[0]] * 1e-3) / 1e9 if ns else None
 
     # e2e through the same C ABI with pinned host output, copies inside the timed region
-    host = torch.empty(max_bytes, dtype=torch.uint8, pin_memory=True)
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = 0 if args.sweep_only else max(1, min(args.steps, 3))
+    host = torch.empty(max_bytes if e2e_steps else 1, dtype=torch.uint8, pin_memory=True)
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -302,14 +327,31 @@ def run_ours(args):
         t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = step_bytes * world * e2e_steps / (e2e_ms * 1e-3) / 1e9
+    e2e_value = step_bytes * world * e2e_steps / (e2e_ms * 1e-3) / 1e9 if e2e_steps else None
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.sweep_only:
         cpu = cpu_baseline_sample(args.cpu_n, calls)
 
+    quasi = config1 = None
+    if rank == 0 and world == 1 and not args.sweep_only:
+        config1 = config1_leg(lib)
+        if not args.no_quasi:
+            del out
+            torch.cuda.empty_cache()
+            out = None
+            quasi = quasi_leg(lib, max(3, min(args.steps, 10)))
+
+    refk = None
+    if rank == 0 and world == 1 and not args.sweep_only and not args.no_ref_kernels:
+        if out is not None:
+            del out
+            out = None
+        torch.cuda.empty_cache()
+        refk = ref_kernels_leg(lib, calls, n, mean_call, 3)
+
     batched = serving = None
-    if rank == 0 and world == 1 and not args.no_batched:
+    if rank == 0 and world == 1 and not args.no_batched and not args.sweep_only:
         del out
         torch.cuda.empty_cache()
         batched = batched_leg(lib, not args.quick_batched)
@@ -324,6 +366,8 @@ def run_ours(args):
 
     if rank != 0:
         return
+    dr = roofs[dom]
+    dom_bytes = dr["bytes"]
     line = {
         "metric": "output GB/s of rocrand_generate_* (bit-exact vs reference host generators)",
         "value": round(value, 2),
@@ -338,35 +382,38 @@ def run_ours(args):
         "dtype": "u32/f32/f64/f16 outputs, int32 engine arithmetic",
         "data": "synthetic: seeded generator streams (seed 0xdeadbeef), no input data",
         "config": {
-            "workload": "plain single-generator sweep, n=2^28 values per call",
-            "generators": [g for g, _ in SWEEP_GENERATORS],
-            "distributions": ["%s%s" % (d, "" if p is None else str(list(p))) for d, p in SWEEP_DISTS],
+            "workload": "plain single-generator sweep, n=2^28 values per call, %d generator families x %d "
+                        "distributions" % (len(SWEEP_GENERATORS), len(SWEEP_DISTS)),
             "n_per_call": n,
             "bytes_per_step_per_gpu": step_bytes,
             "l2": "outputs 0.5-2 GiB per call > 126 MB L2; no flush needed",
             "parallelism": "replica shards: rank r fills stream slice [r*n, (r+1)*n)",
+            "families": ",".join(g for g, _ in SWEEP_GENERATORS),
         },
         "roofline": {
-            "bound": "hbm",
-            "kernel": "%s %s" % (calls[dom][0], calls[dom][2]),
-            "achieved": round(dom_gbs, 1),
-            "peak": peak,
+            "bound": dr["bound"],
+            "kernel": dr["kernel"],
+            "achieved": round(dr["gbs"], 1),
+            "peak": round(min(peak, dr["issue_gbs"]) if dr["issue_gbs"] else peak, 1),
             "unit": "GB/s",
-            "frac": round(dom_gbs / peak, 4),
-            "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs copy bandwidth)" % peak_kind
-            if peak_kind == "measured" else "fallback 6650 GB/s",
+            "frac": round(dr["frac"], 4),
+            "hbm_peak": peak,
+            "hbm_frac": round(dr["hbm_frac"], 4),
+            "issue_frac": round(dr["issue_frac"], 4) if dr["issue_frac"] else None,
+            "peak_source": ("HBM: %s copy bandwidth (MEASURED_PEAKS.json); issue: %s" % (
+                peak_kind, dr["issue_source"])) if peak_kind == "measured" else "fallback 6650 GB/s",
             "traffic": ncu_traffic(calls[dom][0], calls[dom][2], dom_bytes)[0],
             "traffic_source": ncu_traffic(calls[dom][0], calls[dom][2], dom_bytes)[1],
             "algorithmic_bytes_per_launch": dom_bytes,
+            "headline_kernel": ("philox4x32_10 uniform fp32 2^28: %.1f GB/s = %.3f of HBM peak" % (
+                roofs[ns[0]]["gbs"], roofs[ns[0]]["hbm_frac"])) if ns else None,
+            "config1": config1,
+            "quasi_gbs": quasi["gbs"] if quasi else None,
+            "vs_reference_kernels": ({k: refk[k] for k in ("speedup", "min_kernel_speedup", "ours_gbs", "ref_gbs",
+                                                           "identical_bit_exact_outputs")}
+                                     if refk and "speedup" in refk else refk),
         },
-        "philox_uniform_2p28": {"kernel": "philox4x32_10 uniform fp32 n=2^28",
-                       "achieved_gbs": round(ns_gbs, 1) if ns_gbs else None,
-                       "frac_of_peak": round(ns_gbs / peak, 4) if ns_gbs else None,
-                       "traffic": ncu_traffic("philox4x32_10", "uniform", 4 * (1 << 28))[0],
-                       "traffic_source": ncu_traffic("philox4x32_10", "uniform", 4 * (1 << 28))[1]},
-        "per_call_ms": {"%s %s%s" % (c[0], c[2], "" if c[3] is None else list(c[3])): round(mean_call[i], 4)
-                        for i, c in enumerate(calls)},
-        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": step_bytes,
                 "how": "same C-ABI calls + D2H copy of every output to pinned host memory, %d steps" % e2e_steps},
         "gpu_launches": len(calls) * args.steps,
@@ -374,11 +421,166 @@ def run_ours(args):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    # detail: every kernel (device ms, fraction of its governing bound, that bound), then the
+    # short summaries of the other legs last
+    line["per_kernel"] = {r["kernel"]: [round(mean_call[i], 4), round(r["frac"], 3), r["bound"]]
+                          for i, r in enumerate(roofs)}
+    if refk is not None:
+        line["reference_kernels"] = refk
+    if quasi is not None:
+        line["quasi"] = quasi
     if batched is not None:
         line["batched_fill"] = batched
     if serving is not None:
         line["serving"] = serving
     print(json.dumps(line))
+
+
+def quasi_leg(lib, reps):
+    """The quasi-random workload: Sobol32 and scrambled Sobol64, 1 / 64 / 1000 dimensions x
+    2^20 points per dimension at offset 4096, uniform fp64 and normal fp32, dimension-major.
+    Each case: one generator, 2 untimed calls, then `reps` calls timed with CUDA events on
+    its stream (every call continues the sequence).  Output GB/s per case and over all."""
+    import torch
+    import rocrand_b200 as rb
+    stream = torch.cuda.current_stream()
+    out = torch.empty(max(QUASI_DIMS) * (1 << 20) * 8, dtype=torch.uint8, device="cuda")
+    res, tot_b, tot_ms = {}, 0, 0.0
+    for gname, gtype in QUASI_GENERATORS:
+        for dims in QUASI_DIMS:
+            for d, p in QUASI_DISTS:
+                g = c_void_p()
+                rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), gtype))
+                rb.check_rocrand(lib.rocrand_set_quasi_random_generator_dimensions(g, dims))
+                rb.check_rocrand(lib.rocrand_set_offset(g, 4096))
+                rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
+                n = dims << 20
+                fn = getattr(lib, ENTRY[d])
+
+                def call():
+                    st = fn(g, c_void_p(out.data_ptr()), c_size_t(n), *call_args(d, p))
+                    if st != 0:
+                        raise rb.RocRandError(st)
+
+                for _ in range(2):
+                    call()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for _ in range(reps):
+                    call()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                lib.rocrand_destroy_generator(g)
+                b = n * ELEM[d]
+                res["%s/%s/d%d" % (gname, "f64" if d == "uniform_double" else "nf32", dims)] = round(
+                    b / (ms * 1e-3) / 1e9, 1)
+                tot_b += b
+                tot_ms += ms
+    del out
+    return {"gbs": round(tot_b / (tot_ms * 1e-3) / 1e9, 1), "cases": res,
+            "workload": "2^20 points/dim, offset 4096, %d calls each" % reps}
+
+
+def config1_leg(lib):
+    """The small reference case: Philox4x32-10, seed 1234, offset 0, uniform fp32, 2^24 values
+    into a 256-byte aligned buffer -- its SHA-256 against the digest recorded from the
+    reference's own host generator, and its device time."""
+    import hashlib
+    import torch
+    import rocrand_b200 as rb
+    n = 1 << 24
+    with open(os.path.join(HERE, "tests", "golden", "full_digests.json")) as f:
+        want = json.load(f).get("philox/uniform/seed1234/2^24", {}).get("sha256")
+    stream = torch.cuda.current_stream()
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    g = c_void_p()
+    rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), 404))
+    rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
+    times = []
+    for _ in range(6):
+        rb.check_rocrand(lib.rocrand_set_seed(g, 1234))  # every call writes the same values
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rb.check_rocrand(lib.rocrand_generate_uniform(g, c_void_p(out.data_ptr()), c_size_t(n)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    lib.rocrand_destroy_generator(g)
+    got = hashlib.sha256(out.cpu().numpy().view("u1").data).hexdigest()
+    ms = statistics.median(times[1:])
+    return {"bit_exact_vs_reference": got == want, "ms": round(ms, 4),
+            "gbs": round(4 * n / (ms * 1e-3) / 1e9, 1)}
+
+
+REF_GPU_PATH = os.path.join(HERE, "oracle", "_ref", "librocrand_ref_gpu.so")
+BIT_EXACT = {"uint", "uniform", "uniform_double", "uniform_half", "poisson"}
+
+
+def ref_kernels_leg(lib, calls, n, ours_ms, reps):
+    """The reference's own device kernels on the same B200: its sources compiled for sm_100a
+    (oracle/_ref/librocrand_ref_gpu.so, built by oracle/Makefile.ref gpu), the same sweep
+    through its own rocrand_generate_* entry points, each call timed with CUDA events like
+    ours.  Per kernel: our time and the reference's; bit-exact outputs of the first call on
+    fresh generators are compared byte for byte."""
+    import torch
+    import rocrand_b200 as rb
+    if not os.path.exists(REF_GPU_PATH):
+        return {"unavailable": "oracle/_ref/librocrand_ref_gpu.so not built"}
+    ref = rb.load_library(REF_GPU_PATH)
+    stream = torch.cuda.current_stream()
+    nbytes = max(ELEM[d] for _, _, d, _ in calls) * n
+    a = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    b = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    per, same, compared, ours_tot, ref_tot = {}, 0, 0, 0.0, 0.0
+    for i, (gname, gtype, d, p) in enumerate(calls):
+        ms = []
+        for k, (L, buf) in enumerate(((lib, a), (ref, b))):
+            g = c_void_p()
+            rb.check_rocrand(L.rocrand_create_generator(ctypes.byref(g), gtype))
+            rb.check_rocrand(L.rocrand_set_seed(g, SEED))
+            rb.check_rocrand(L.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
+            fn = getattr(L, ENTRY[d])
+            rb.check_rocrand(fn(g, c_void_p(buf.data_ptr()), c_size_t(n), *call_args(d, p)))
+            if k == 1 and d in BIT_EXACT:
+                torch.cuda.synchronize()
+                nb = ELEM[d] * n
+                compared += 1
+                same += int(torch.equal(a[:nb], b[:nb]))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                rb.check_rocrand(fn(g, c_void_p(buf.data_ptr()), c_size_t(n), *call_args(d, p)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1) / reps)
+            L.rocrand_destroy_generator(g)
+        key = "%s %s%s" % (gname, d, "" if p is None else list(p))
+        per[key] = [round(ms[0], 4), round(ms[1], 4), round(ms[1] / ms[0], 2)]
+        ours_tot += ms[0]
+        ref_tot += ms[1]
+    del a, b
+    torch.cuda.empty_cache()
+    step_bytes = sum(ELEM[d] * n for _, _, d, _ in calls)
+    ratios = sorted(v[2] for v in per.values())
+    return {"ours_gbs": round(step_bytes / (ours_tot * 1e-3) / 1e9, 1),
+            "ref_gbs": round(step_bytes / (ref_tot * 1e-3) / 1e9, 1),
+            "speedup": round(ref_tot / ours_tot, 2),
+            "min_kernel_speedup": ratios[0], "median_kernel_speedup": ratios[len(ratios) // 2],
+            "identical_bit_exact_outputs": "%d of %d" % (same, compared),
+            "per_kernel_ms_ours_ref_ratio": per}
+
+
+def issue_bound(gname, dist, n, clock_mhz):
+    """(GB/s that the instruction issue rate allows, source) for one sweep kernel: warp
+    instructions per output value from the ncu capture in NCU_INST, issued at most 4 per SM
+    per clock on 148 SMs at the sampled SM clock; (None, None) where no capture exists."""
+    per_value = NCU_INST.get((gname, dist))
+    if per_value is None or not clock_mhz:
+        return None, None
+    secs = per_value * n / (148 * 4 * clock_mhz * 1e6)
+    return ELEM[dist] * n / secs / 1e9, "%s: %.3f warp instructions per value" % (NCU_INST_SOURCE, per_value)
 
 
 # ------------------------------------------------------------------------------------
@@ -626,10 +828,13 @@ def cpu_sample(n_per_call, calls, threads):
 def cpu_baseline_sample(n_per_call, calls):
     threads = os.cpu_count() or 1
     nb, secs, kind = cpu_sample(n_per_call, calls, threads)
+    one_n = max(1 << 16, n_per_call // 16)
+    nb1, secs1, _ = cpu_sample(one_n, calls, 1)
     return {"value": round(nb / secs / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-            "sample": "same sweep at n=%d values per call (vs 2^28 on the GPU), %d host threads, "
-                      "each its own host generator on a disjoint offset slice (MT19937, MTGP32: own "
-                      "seed; MT19937 from the C port)" % (n_per_call, threads)}
+            "value_1core": round(nb1 / secs1 / 1e9, 4),
+            "sample": "same sweep at n=%d values per call (1 core: n=%d) vs 2^28 on the GPU; "
+                      "%d host threads, each its own host generator on a disjoint offset slice" % (
+                          n_per_call, one_n, threads)}
 
 
 def run_reference(args):
@@ -682,6 +887,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="", help="gen:dist[:param],... subset of the sweep")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-fill and serving legs")
+    ap.add_argument("--no-quasi", action="store_true", help="skip the quasi-random (Sobol) leg")
+    ap.add_argument("--no-ref-kernels", action="store_true",
+                    help="skip timing the reference's own device kernels (oracle/_ref gpu build)")
+    ap.add_argument("--sweep-only", action="store_true",
+                    help="only the timed sweep (no e2e, CPU, config-1, quasi, batched or serving legs): "
+                         "the form profiled under ncu")
     ap.add_argument("--full-configs", action="store_true", help="serving with 10^5 requests per rate")
     ap.add_argument("--quick-batched", action="store_true",
                     help="batched-fill leg on 1024 + 1024 generators instead of 4096 + 4096")

@@ -298,18 +298,64 @@ __device__ __forceinline__ void unit_values(const F& f, const uint32_t (&r)[kMtS
     f(in, out);
 }
 
+// Where a thread's input units come from in a round.  RegUnits reads its 78 slots in
+// registers.  SharedUnits reads them from shared memory, where the kernel staged them after
+// the twist: with the state out of registers, the long fp64 transforms (about 170 fp64
+// operations per Box-Muller pair) get the registers to run several independent pairs at once,
+// which the 14 warps per SM that hold all 65536 lanes cannot hide on their own.
+template<class F>
+struct RegUnits
+{
+    using Fn = F;
+    const F&        f;
+    const uint32_t (&r)[kMtSlots];
+    template<unsigned G>
+    __device__ __forceinline__ void get(typename F::T (&out)[F::ow]) const
+    {
+        unit_values<G>(f, r, out);
+    }
+};
+
+template<class F>
+struct SharedUnits
+{
+    using Fn = F;
+    const F&        f;
+    const uint32_t* s; // slot j of this thread at s[j * kMtBlock]
+    template<unsigned G>
+    __device__ __forceinline__ void get(typename F::T (&out)[F::ow]) const
+    {
+        uint32_t in[F::iw];
+#pragma unroll
+        for(unsigned i = 0; i < F::iw; i++)
+            in[i] = mt_temper(s[(G * F::iw + i) * kMtBlock]);
+        f(in, out);
+    }
+};
+
+// Transforms long enough that the state is staged through shared memory for them.
+template<class F>
+constexpr bool kMtStaged = std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value;
+
+// Shared memory of one block of mt_fill: the distribution's table, or the staged state.
+template<class F>
+inline size_t mt_fill_smem(const F& f)
+{
+    return kMtStaged<F> ? sizeof(uint32_t) * kMtSlots * kMtBlock : table_smem_bytes(f);
+}
+
 // A round whose units all lie inside the call: every slot group is stored.
-template<class F, unsigned... G>
-__device__ __forceinline__ void round_interior(const F& f, const uint32_t (&r)[kMtSlots],
-                                               const MtArgs& a, long long q0,
+template<class U, unsigned... G>
+__device__ __forceinline__ void round_interior(const U& u, const MtArgs& a, long long q0,
                                                std::integer_sequence<unsigned, G...>)
 {
-    using T               = typename F::T;
-    constexpr unsigned VB = sizeof(T) * F::ow;
+    using T               = typename U::Fn::T;
+    constexpr unsigned ow = U::Fn::ow;
+    constexpr unsigned VB = sizeof(T) * ow;
     (
         [&] {
-            T out[F::ow];
-            unit_values<G>(f, r, out);
+            T out[ow];
+            u.template get<G>(out);
             store_vec(a.vec + static_cast<unsigned long long>(q0 + G * kMtThreads) * VB, out);
         }(),
         ...);
@@ -317,20 +363,20 @@ __device__ __forceinline__ void round_interior(const F& f, const uint32_t (&r)[k
 
 // The first or last round of a call: units outside the call are skipped, and the one
 // extra unit writes the head and tail.
-template<class F, unsigned... G>
-__device__ __forceinline__ void round_edge(const F& f, const uint32_t (&r)[kMtSlots], const MtArgs& a,
-                                           long long q0, std::integer_sequence<unsigned, G...>)
+template<class U, unsigned... G>
+__device__ __forceinline__ void round_edge(const U& u, const MtArgs& a, long long q0,
+                                           std::integer_sequence<unsigned, G...>)
 {
-    using T               = typename F::T;
-    constexpr unsigned VB = sizeof(T) * F::ow;
-    constexpr unsigned ow = F::ow;
+    using T               = typename U::Fn::T;
+    constexpr unsigned ow = U::Fn::ow;
+    constexpr unsigned VB = sizeof(T) * ow;
     (
         [&] {
             const long long q = q0 + static_cast<long long>(G) * kMtThreads;
             if(q < 0 || static_cast<unsigned long long>(q) >= a.total)
                 return;
             T out[ow];
-            unit_values<G>(f, r, out);
+            u.template get<G>(out);
             if(static_cast<unsigned long long>(q) < a.vec_n)
             {
                 store_vec(a.vec + static_cast<unsigned long long>(q) * VB, out);
@@ -351,15 +397,28 @@ __device__ __forceinline__ void round_edge(const F& f, const uint32_t (&r)[kMtSl
         ...);
 }
 
+template<class U>
+__device__ __forceinline__ void mt_round(const U& u, const MtArgs& a, uint32_t rho)
+{
+    constexpr unsigned per = kMtSlots / U::Fn::iw;
+    using Groups           = std::make_integer_sequence<unsigned, per>;
+    const unsigned tid     = blockIdx.x * kMtBlock + threadIdx.x;
+    // q of slot group 0 for thread 0 of this round (negative before the call's start)
+    const long long base = static_cast<long long>(rho) * a.full - a.start;
+    const long long q0   = base + tid;
+    if(base >= 0 && static_cast<unsigned long long>(base) + a.full <= a.total)
+        round_interior(u, a, q0, Groups{});
+    else
+        round_edge(u, a, q0, Groups{});
+}
+
 template<class F>
 __global__ __launch_bounds__(kMtBlock, 7) void mt_fill(MtArgs a, F fw)
 {
     extern __shared__ unsigned char smem[];
-    const F            f    = stage_table(fw, smem);
-    const unsigned     tid  = blockIdx.x * kMtBlock + threadIdx.x;
-    const unsigned     lane = threadIdx.x & 7u;
-    constexpr unsigned per  = kMtSlots / F::iw;
-    using Groups            = std::make_integer_sequence<unsigned, per>;
+    const F        f    = stage_table(fw, smem);
+    const unsigned tid  = blockIdx.x * kMtBlock + threadIdx.x;
+    const unsigned lane = threadIdx.x & 7u;
 
     uint32_t r[kMtSlots];
 #pragma unroll
@@ -370,13 +429,25 @@ __global__ __launch_bounds__(kMtBlock, 7) void mt_fill(MtArgs a, F fw)
     {
         if(rho > 0 || a.twist_first)
             mt_twist(r, lane);
-        // q of slot group 0 for thread 0 of this round (negative before the call's start)
-        const long long base = static_cast<long long>(rho) * a.full - a.start;
-        const long long q0   = base + tid;
-        if(base >= 0 && static_cast<unsigned long long>(base) + a.full <= a.total)
-            round_interior(f, r, a, q0, Groups{});
+        if constexpr(kMtStaged<F>)
+        {
+            // the thread's own slots, one bank each (slot j of thread t at word j * 64 + t)
+            uint32_t* s = reinterpret_cast<uint32_t*>(smem) + threadIdx.x;
+#pragma unroll
+            for(unsigned j = 0; j < kMtSlots; j++)
+                s[j * kMtBlock] = r[j];
+            // the registers are dead from here: the compiler must read the slots back
+            asm volatile("" ::: "memory");
+            mt_round(SharedUnits<F>{f, s}, a, rho);
+            asm volatile("" ::: "memory");
+#pragma unroll
+            for(unsigned j = 0; j < kMtSlots; j++)
+                r[j] = s[j * kMtBlock];
+        }
         else
-            round_edge(f, r, a, q0, Groups{});
+        {
+            mt_round(RegUnits<F>{f, r}, a, rho);
+        }
     }
     if(a.rounds > 1 || (a.rounds == 1 && a.twist_first))
     {
@@ -555,7 +626,7 @@ private:
                                      : static_cast<uint32_t>((m_start + a.total - 1) / full + 1);
         if(a.total > 0)
         {
-            const size_t smem = table_smem_bytes(f);
+            const size_t smem = mt_fill_smem(f);
             mt_fill<F><<<kMtThreads / kMtBlock, kMtBlock, smem, m_stream>>>(a, f);
             const rocrand_status st = launch_status();
             if(st != ROCRAND_STATUS_SUCCESS)

@@ -34,6 +34,9 @@ QUASI_OFFSET = 4096
 
 
 def cases():
+    # the small reference case: Philox4x32-10, seed 1234, uniform fp32, 2^24 values
+    yield {"key": "philox/uniform/seed1234/2^24", "rng": PSEUDO["philox"], "seed": 1234, "offset": None,
+           "dims": None, "call": ["uniform", 1 << 24, [], 0]}
     for name in sorted(PSEUDO):
         for dist in ("uniform", "uint"):
             yield {"key": "%s/%s/2^28" % (name, dist), "rng": PSEUDO[name], "seed": 0xdeadbeef,
