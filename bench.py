@@ -14,11 +14,10 @@ cpu_baseline = the reference's own host generators (oracle/_ref, compiled from t
          sources) on this host's cores, on a bounded sample of the same sweep.
 
 --impl reference runs only the reference's CPU host generators on the same workload.
-Multi-GPU (torchrun): each rank fills its own slice [r*n, (r+1)*n) of every stream by
-offset (rank_stream), no data-path collective; weak scaling.  Where an offset cannot select
-that slice -- MT19937 and MTGP32 have no offset, and a stateful engine consuming two values per output
-maps offset and output positions differently -- rank r uses seed 0xdeadbeef + r instead
-(an independent stream of the same size).
+Multi-GPU (torchrun): each rank fills its own slice [r*n, (r+1)*n) of every stream through
+rocrand_b200_set_output_position (rank_stream), no data-path collective; weak scaling.
+MT19937 and MTGP32 have no position: rank r uses seed 0xdeadbeef + r instead (an
+independent stream of the same size).
 """
 
 import argparse
@@ -79,14 +78,18 @@ def ncu_traffic(gname, dist, out_bytes):
     return int(read + out_bytes), "%s: state read %.2f MB per launch + the output written once" % (source, read / 1e6)
 
 
+OUTPUT_KIND = {"uint": 0, "uniform": 4, "uniform_double": 5, "uniform_half": 6, "normal": 7,
+               "normal_double": 8, "log_normal": 10, "poisson": 13, "char": 1, "short": 2}
+
+
 def rank_stream(gtype, dist, rank, n):
-    """(seed, offset or None) giving rank `rank` the outputs [rank*n, (rank+1)*n) of the
-    stream of seed SEED.  Counter engines, and stateful engines at one engine value per
-    output, continue the stream at an offset (out_offset[i] = out_0[offset + i]); MT19937,
-    MTGP32 and two-value stateful distributions take seed SEED + rank instead."""
-    if gtype in NO_OFFSET or (gtype in STATEFUL and dist in TWO_WORD):
+    """(seed, output position or None) giving rank `rank` the outputs [rank*n, (rank+1)*n) of
+    the stream of seed SEED: every generator with a position (counter and stateful engines,
+    rocrand_b200_set_output_position) continues that one stream at output rank*n; MT19937
+    and MTGP32, which have no position, take seed SEED + rank instead."""
+    if gtype in NO_OFFSET:
         return SEED + rank, None
-    return SEED, stream_offset(dist, rank * n)
+    return SEED, rank * n
 SWEEP_DISTS = [
     ("uint", None), ("uniform", None), ("uniform_double", None), ("uniform_half", None),
     ("normal", (0.0, 1.0)), ("normal_double", (0.0, 1.0)), ("log_normal", (0.0, 1.0)),
@@ -240,10 +243,10 @@ def run_ours(args):
     for gname, gtype, d, p in calls:
         g = c_void_p()
         rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), gtype))
-        seed, offset = rank_stream(gtype, d, rank, n)
+        seed, pos = rank_stream(gtype, d, rank, n)
         rb.check_rocrand(lib.rocrand_set_seed(g, seed))
-        if offset is not None:
-            rb.check_rocrand(lib.rocrand_set_offset(g, offset))
+        if pos is not None and pos > 0:
+            rb.check_rocrand(lib.rocrand_b200_set_output_position(g, OUTPUT_KIND[d], pos))
         rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
         gens[(gname, d, p)] = g
 
@@ -534,20 +537,33 @@ def ref_kernels_leg(lib, calls, n, ours_ms, reps):
     a = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     b = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     per, same, compared, ours_tot, ref_tot = {}, 0, 0, 0.0, 0.0
+    ulps = {}
     for i, (gname, gtype, d, p) in enumerate(calls):
-        ms = []
-        for k, (L, buf) in enumerate(((lib, a), (ref, b))):
+        gens, fns = [], []
+        for L, buf in ((lib, a), (ref, b)):
             g = c_void_p()
             rb.check_rocrand(L.rocrand_create_generator(ctypes.byref(g), gtype))
             rb.check_rocrand(L.rocrand_set_seed(g, SEED))
             rb.check_rocrand(L.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
             fn = getattr(L, ENTRY[d])
+            # first call on a fresh generator: the outputs compared below
             rb.check_rocrand(fn(g, c_void_p(buf.data_ptr()), c_size_t(n), *call_args(d, p)))
-            if k == 1 and d in BIT_EXACT:
-                torch.cuda.synchronize()
-                nb = ELEM[d] * n
-                compared += 1
-                same += int(torch.equal(a[:nb], b[:nb]))
+            gens.append((L, g))
+            fns.append((fn, buf))
+        torch.cuda.synchronize()
+        nb = ELEM[d] * n
+        if d in BIT_EXACT:
+            compared += 1
+            same += int(torch.equal(a[:nb], b[:nb]))
+        elif d in ("normal", "normal_double"):
+            # distance of the reference kernel's normals from ours (ours are within the stated
+            # ulp bound of the reference's host generator), in ulps of the output
+            it = torch.int32 if d == "normal" else torch.int64
+            x, y = a[:nb].view(it), b[:nb].view(it)
+            same_sign = (x >= 0) == (y >= 0)
+            ulps["%s %s" % (gname, d)] = int((x - y).abs()[same_sign].max().item())
+        ms = []
+        for (L, g), (fn, buf) in zip(gens, fns):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(reps):
@@ -569,6 +585,7 @@ def ref_kernels_leg(lib, calls, n, ours_ms, reps):
             "speedup": round(ref_tot / ours_tot, 2),
             "min_kernel_speedup": ratios[0], "median_kernel_speedup": ratios[len(ratios) // 2],
             "identical_bit_exact_outputs": "%d of %d" % (same, compared),
+            "ref_normal_max_ulps_from_ours": ulps,
             "per_kernel_ms_ours_ref_ratio": per}
 
 
@@ -695,59 +712,115 @@ def batched_leg(lib, full):
             "mix": "50% uniform fp32 / 30% normal fp32 / 20% Poisson 4"}
 
 
+def serving_rates(lib, types):
+    """Per-request costs of plain calls, for the bound of the batched/plain ratio: the device
+    throughput of each (generator, dtype) at 2^24 values, and the wall time per call of
+    back-to-back tiny calls on one stream (the launch floor a per-request server pays)."""
+    import torch
+    import rocrand_b200 as rb
+    stream = torch.cuda.current_stream()
+    buf = torch.empty(8 << 24, dtype=torch.uint8, device="cuda")
+    entries = {0: "rocrand_generate", 1: "rocrand_generate_uniform", 2: "rocrand_generate_uniform_double"}
+    bw, floor = {}, None
+    for t in types:
+        g = c_void_p()
+        rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), t))
+        rb.check_rocrand(lib.rocrand_set_stream(g, c_void_p(stream.cuda_stream)))
+        for d, fname in entries.items():
+            fn = getattr(lib, fname)
+            n = 1 << 24
+            for _ in range(2):
+                fn(g, c_void_p(buf.data_ptr()), c_size_t(n))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(5):
+                fn(g, c_void_p(buf.data_ptr()), c_size_t(n))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            bw[(t, d)] = n * (8 if d == 2 else 4) / (e0.elapsed_time(e1) / 5 * 1e-3)
+        if t == types[0]:
+            fn = lib.rocrand_generate_uniform
+            for _ in range(50):
+                fn(g, c_void_p(buf.data_ptr()), c_size_t(256))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(1000):
+                fn(g, c_void_p(buf.data_ptr()), c_size_t(256))
+            torch.cuda.synchronize()
+            floor = (time.perf_counter() - t0) / 1000
+        lib.rocrand_destroy_generator(g)
+    del buf
+    return bw, floor
+
+
 def serving_leg(lib, full):
     """Serving: Poisson arrivals at 1k-50k req/s over 64 handles (16 each of Philox,
     XORWOW, MRG32k3a, Sobol32; states resident), sizes log-uniform in [2^8, 2^26], dtypes
     uniform over fp32 / fp64 / uint32, a 64 GB output budget; the continuous-batching server
     and the plain per-request server replay the same trace.  Also a saturated trace (every
-    request at t=0).  Requests per rate: 10^5 with --full-configs, else 2000."""
+    request at t=0).  Requests per trace: 10^5 at 50k req/s, 2000 otherwise (10^5 at every
+    rate with --full-configs).  For the saturated trace the report includes the bound of the
+    batched/plain ratio that the mix allows: sum over requests of max(launch floor, device
+    time) / sum of device times (serving_rates)."""
     import numpy as np
     import rocrand_b200 as rb
     types = [rb.ROCRAND_RNG_PSEUDO_PHILOX4_32_10, rb.ROCRAND_RNG_PSEUDO_XORWOW,
              rb.ROCRAND_RNG_PSEUDO_MRG32K3A, rb.ROCRAND_RNG_QUASI_SOBOL32]
-    nreq = 100000 if full else 2000
     budget = 64 << 30
     rates = [1000, 5000, 10000, 20000, 50000, None]
+    bw, floor = serving_rates(lib, types)
     results = {}
     for mode in ("batched", "plain"):
         server = c_void_p()
         rb.check_rocrand(lib.rocrand_b200_server_create(ctypes.byref(server), budget, 3,
                                                         1 if mode == "plain" else 0))
         handles = []
+        htype = []
         for t in types:
             for k in range(16):
                 h = ctypes.c_uint()
                 rb.check_rocrand(lib.rocrand_b200_server_add_generator(server, t, splitmix64(len(handles)),
                                                                        ctypes.byref(h)))
                 handles.append(h.value)
+                htype.append(t)
         for rate in rates:
             rs = np.random.Generator(np.random.PCG64(7))
-            n = nreq if rate is None or rate >= 5000 or full else min(nreq, 1000)
+            n = 100000 if (full or rate == 50000) else (2000 if (rate is None or rate >= 5000) else 1000)
             gaps = rs.exponential(1.0 / rate, n) if rate else np.zeros(n)
             arrivals = np.cumsum(gaps) if rate else gaps
             hidx = rs.integers(0, len(handles), n)
             dts = rs.integers(0, 3, n)  # uint32, fp32, fp64
             sizes = np.exp(rs.uniform(np.log(2.0 ** 8), np.log(2.0 ** 26), n)).astype(np.int64)
             items = (rb.TraceItem * n)()
-            dist_of = {0: 0, 1: 1, 2: 2}
             nbytes = 0
+            dev_s = plain_s = 0.0
             for i in range(n):
-                items[i] = rb.TraceItem(float(arrivals[i]), handles[hidx[i]], dist_of[int(dts[i])], 0.0, 0.0,
+                items[i] = rb.TraceItem(float(arrivals[i]), handles[hidx[i]], int(dts[i]), 0.0, 0.0,
                                         int(sizes[i]))
-                nbytes += int(sizes[i]) * (8 if dts[i] == 2 else 4)
+                b = int(sizes[i]) * (8 if dts[i] == 2 else 4)
+                nbytes += b
+                t_dev = b / bw[(htype[hidx[i]], int(dts[i]))]
+                dev_s += t_dev
+                plain_s += max(floor, t_dev)
             lat = (ctypes.c_double * n)()
             wall = ctypes.c_double()
             rb.check_rocrand(lib.rocrand_b200_server_run_trace(server, items, n, lat, ctypes.byref(wall)))
             l = np.ctypeslib.as_array(lat)
             key = "saturated" if rate is None else "%d_req_s" % rate
-            results.setdefault(key, {"requests": n})[mode] = {
-                "gbs": round(nbytes / wall.value / 1e9, 1), "p50_ms": round(float(np.percentile(l, 50)) * 1e3, 3),
-                "p99_ms": round(float(np.percentile(l, 99)) * 1e3, 3), "wall_s": round(wall.value, 3)}
+            ent = results.setdefault(key, {"requests": n})
+            ent[mode] = {"gbs": round(nbytes / wall.value / 1e9, 1),
+                         "p50_ms": round(float(np.percentile(l, 50)) * 1e3, 3),
+                         "p99_ms": round(float(np.percentile(l, 99)) * 1e3, 3), "wall_s": round(wall.value, 3)}
+            if rate is None:
+                ent["ratio_bound"] = round(plain_s / dev_s, 3)
+                ent["kernel_time_s"] = round(dev_s, 3)
         rb.check_rocrand(lib.rocrand_b200_server_destroy(server))
     for v in results.values():
         if "batched" in v and "plain" in v:
-            v["gbs_ratio"] = round(v["batched"]["gbs"] / v["plain"]["gbs"], 2)
-    return {"budget_bytes": budget, "handles": 64, "streams": 3,
+            v["gbs_ratio"] = round(v["batched"]["gbs"] / v["plain"]["gbs"], 3)
+            if "ratio_bound" in v:
+                v["of_bound"] = round(v["gbs_ratio"] / v["ratio_bound"], 3)
+    return {"budget_bytes": budget, "handles": 64, "streams": 3, "launch_floor_us": round(floor * 1e6, 2),
             "sizes": "log-uniform [2^8, 2^26]", "dtypes": "uint32/fp32/fp64", "rates": results}
 
 

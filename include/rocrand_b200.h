@@ -37,6 +37,49 @@ rocrand_status ROCRANDAPI rocrand_b200_generate_poisson_noalloc(unsigned long lo
                                                                 hipStream_t        stream);
 
 /*
+ * Output position, for sharding one stream over several GPUs or processes.  No counterpart
+ * in the reference.
+ *
+ * The outputs of one rocrand_generate_* call of kind `output` are positioned at `index` of
+ * the stream that a fresh generator of the same type and seed writes with that kind in one
+ * call from offset 0: after this call, the next call of that kind writes exactly outputs
+ * [index, index + n) of that single stream (into an output aligned like the single call's).
+ * Rank r of N, each calling it with index = r * n before generating n outputs, therefore
+ * writes slice r of one stream, with no communication.
+ *  - XORWOW, MRG32k3a, MRG31k3p, LFSR113: output vector V = index / w (w outputs of iw
+ *    engine values each, per the distribution) was served by engine V mod 131072, so every
+ *    engine e is placed after iw * (V / 131072 + (e < V mod 131072)) values and the engine
+ *    rotation starts at V mod 131072 -- a placement rocrand_set_offset cannot express when
+ *    iw > 1 or w > 1 (uniform double, normal and log-normal outputs);
+ *  - Philox4x32-10 and ThreeFry: the offset index / w * iw (rocrand_set_offset);
+ *  - MT19937, MTGP32 and the quasi-random generators: ROCRAND_STATUS_TYPE_ERROR (they have
+ *    no offset);
+ * index not a multiple of w gives ROCRAND_STATUS_LENGTH_NOT_MULTIPLE.  The position replaces
+ * any offset; a later rocrand_set_offset replaces the position.
+ */
+typedef enum rocrand_b200_output
+{
+    ROCRAND_B200_OUTPUT_UINT              = 0,  /* rocrand_generate */
+    ROCRAND_B200_OUTPUT_UCHAR             = 1,  /* rocrand_generate_char */
+    ROCRAND_B200_OUTPUT_USHORT            = 2,  /* rocrand_generate_short */
+    ROCRAND_B200_OUTPUT_ULONGLONG         = 3,  /* rocrand_generate_long_long */
+    ROCRAND_B200_OUTPUT_UNIFORM_FLOAT     = 4,  /* rocrand_generate_uniform */
+    ROCRAND_B200_OUTPUT_UNIFORM_DOUBLE    = 5,  /* rocrand_generate_uniform_double */
+    ROCRAND_B200_OUTPUT_UNIFORM_HALF      = 6,  /* rocrand_generate_uniform_half */
+    ROCRAND_B200_OUTPUT_NORMAL_FLOAT      = 7,  /* rocrand_generate_normal */
+    ROCRAND_B200_OUTPUT_NORMAL_DOUBLE     = 8,  /* rocrand_generate_normal_double */
+    ROCRAND_B200_OUTPUT_NORMAL_HALF       = 9,  /* rocrand_generate_normal_half */
+    ROCRAND_B200_OUTPUT_LOG_NORMAL_FLOAT  = 10, /* rocrand_generate_log_normal */
+    ROCRAND_B200_OUTPUT_LOG_NORMAL_DOUBLE = 11, /* rocrand_generate_log_normal_double */
+    ROCRAND_B200_OUTPUT_LOG_NORMAL_HALF   = 12, /* rocrand_generate_log_normal_half */
+    ROCRAND_B200_OUTPUT_POISSON           = 13  /* rocrand_generate_poisson */
+} rocrand_b200_output;
+
+rocrand_status ROCRANDAPI rocrand_b200_set_output_position(rocrand_generator   generator,
+                                                           rocrand_b200_output output,
+                                                           unsigned long long  index);
+
+/*
  * Batched fill.  No counterpart in the reference.
  *
  * A request is exactly one plain generate call on a fresh generator: rng_type created,

@@ -103,6 +103,7 @@ _SIGNATURES = [
     ("rocrand_b200_server_wait", [c_void_p, ctypes.c_ulonglong, c_void_p, c_void_p]),
     ("rocrand_b200_server_release", [c_void_p, ctypes.c_ulonglong]),
     ("rocrand_b200_server_run_trace", [c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
+    ("rocrand_b200_set_output_position", [_G, c_int, c_ulonglong]),
     ("rocrand_create_generator", [POINTER(c_void_p), c_int]),
     ("rocrand_create_generator_host", [POINTER(c_void_p), c_int]),
     ("rocrand_create_generator_host_blocking", [POINTER(c_void_p), c_int]),

@@ -7,6 +7,8 @@
 #include "common.hpp"
 #include "generators.hpp"
 
+#include <rocrand_b200.h>
+
 #include <cuda_fp16.h>
 
 #include <new>
@@ -296,6 +298,18 @@ rocrand_status ROCRANDAPI rocrand_set_seed_uint4(rocrand_generator generator, ui
 rocrand_status ROCRANDAPI rocrand_set_offset(rocrand_generator generator, unsigned long long offset)
 {
     RB200_GEN(generator, generator->set_offset(offset));
+}
+
+// Addition of this library (include/rocrand_b200.h): no counterpart in the reference.
+rocrand_status ROCRANDAPI rocrand_b200_set_output_position(rocrand_generator   generator,
+                                                           rocrand_b200_output output,
+                                                           unsigned long long  index)
+{
+    if(generator == nullptr)
+        return ROCRAND_STATUS_NOT_CREATED;
+    if(static_cast<int>(output) < 0 || static_cast<int>(output) > static_cast<int>(Dist::POISSON))
+        return ROCRAND_STATUS_OUT_OF_RANGE;
+    return guarded([&] { return generator->set_output_position(static_cast<Dist>(output), index); });
 }
 
 rocrand_status ROCRANDAPI rocrand_set_ordering(rocrand_generator generator, rocrand_ordering order)

@@ -115,6 +115,14 @@ struct rocrand_generator_base_type
         m_stream = stream;
         return ROCRAND_STATUS_SUCCESS;
     }
+    // Positions the generator at output `index` of the stream that a fresh generator of the
+    // same type and seed (offset 0) writes with distribution d in one call, so that the next
+    // call of d continues that stream from there (rocrand_b200_set_output_position).
+    virtual rocrand_status set_output_position(rb200::Dist d, unsigned long long index)
+    {
+        (void)d, (void)index;
+        return ROCRAND_STATUS_TYPE_ERROR;
+    }
     // One generate call: data is device memory of n elements of the distribution's type.
     virtual rocrand_status generate(void* data, size_t n, rb200::Dist d, const rb200::DistParams& p)
         = 0;

@@ -41,6 +41,7 @@ public:
     ~PhiloxGenerator() override;
     rocrand_rng_type type() const override { return ROCRAND_RNG_PSEUDO_PHILOX4_32_10; }
     rocrand_status   init() override;
+    rocrand_status   set_output_position(rb200::Dist d, unsigned long long index) override;
     rocrand_status   set_order(rocrand_ordering order) override;
     rocrand_status   generate(void* data, size_t n, Dist d, const DistParams& p) override;
     rocrand_status   generate_poisson(unsigned int* data, size_t n, double lambda) override;

@@ -298,11 +298,8 @@ __device__ __forceinline__ void unit_values(const F& f, const uint32_t (&r)[kMtS
     f(in, out);
 }
 
-// Where a thread's input units come from in a round.  RegUnits reads its 78 slots in
-// registers.  SharedUnits reads them from shared memory, where the kernel staged them after
-// the twist: with the state out of registers, the long fp64 transforms (about 170 fp64
-// operations per Box-Muller pair) get the registers to run several independent pairs at once,
-// which the 14 warps per SM that hold all 65536 lanes cannot hide on their own.
+// A thread's input units of a round, from its 78 slots in registers (the short transforms;
+// the long ones are staged through shared memory, mt_round_staged).
 template<class F>
 struct RegUnits
 {
@@ -316,26 +313,12 @@ struct RegUnits
     }
 };
 
+// Transforms long enough that the state is staged through shared memory for them (the
+// normal and log-normal outputs: Box-Muller on every pair).
 template<class F>
-struct SharedUnits
-{
-    using Fn = F;
-    const F&        f;
-    const uint32_t* s; // slot j of this thread at s[j * kMtBlock]
-    template<unsigned G>
-    __device__ __forceinline__ void get(typename F::T (&out)[F::ow]) const
-    {
-        uint32_t in[F::iw];
-#pragma unroll
-        for(unsigned i = 0; i < F::iw; i++)
-            in[i] = mt_temper(s[(G * F::iw + i) * kMtBlock]);
-        f(in, out);
-    }
-};
-
-// Transforms long enough that the state is staged through shared memory for them.
-template<class F>
-constexpr bool kMtStaged = std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value;
+constexpr bool kMtStaged = std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value
+                           || std::is_same<F, FnNormalF>::value || std::is_same<F, FnLogNormalF>::value
+                           || std::is_same<F, FnNormalH>::value || std::is_same<F, FnLogNormalH>::value;
 
 // Shared memory of one block of mt_fill: the distribution's table, or the staged state.
 template<class F>
@@ -397,6 +380,51 @@ __device__ __forceinline__ void round_edge(const U& u, const MtArgs& a, long lon
         ...);
 }
 
+// A round whose slots were staged in shared memory (slot j of this thread at s[j * 64]):
+// the slot groups are a loop, not an unrolled sequence, so one copy of the transform (two,
+// for two independent pairs in flight) stays in the instruction cache.
+template<class F>
+__device__ __forceinline__ void mt_round_staged(const F& f, const uint32_t* s, const MtArgs& a, uint32_t rho)
+{
+    using T                = typename F::T;
+    constexpr unsigned per = kMtSlots / F::iw;
+    constexpr unsigned ow  = F::ow;
+    constexpr unsigned VB  = sizeof(T) * ow;
+    const unsigned     tid = blockIdx.x * kMtBlock + threadIdx.x;
+    const long long    base = static_cast<long long>(rho) * a.full - a.start;
+    const long long    q0   = base + tid;
+    const bool interior = base >= 0 && static_cast<unsigned long long>(base) + a.full <= a.total;
+#pragma unroll 2
+    for(unsigned G = 0; G < per; G++)
+    {
+        const long long q = q0 + static_cast<long long>(G) * kMtThreads;
+        if(!interior && (q < 0 || static_cast<unsigned long long>(q) >= a.total))
+            continue;
+        uint32_t in[F::iw];
+#pragma unroll
+        for(unsigned i = 0; i < F::iw; i++)
+            in[i] = mt_temper(s[(G * F::iw + i) * kMtBlock]);
+        T out[ow];
+        f(in, out);
+        if(interior || static_cast<unsigned long long>(q) < a.vec_n)
+        {
+            store_vec(a.vec + static_cast<unsigned long long>(q) * VB, out);
+            continue;
+        }
+        // the extra unit: head from its front, tail from its back, the tail written
+        // downwards from the end (mt19937.hpp:404-430)
+        T* data = reinterpret_cast<T*>(a.data);
+#pragma unroll
+        for(unsigned o = 0; o < ow; o++)
+        {
+            if(o < a.head)
+                data[o] = out[o];
+            if(static_cast<int>(o) > static_cast<int>(ow) - static_cast<int>(a.tail) - 1)
+                data[a.n + (ow - a.tail - 1) - o] = out[o];
+        }
+    }
+}
+
 template<class U>
 __device__ __forceinline__ void mt_round(const U& u, const MtArgs& a, uint32_t rho)
 {
@@ -438,7 +466,7 @@ __global__ __launch_bounds__(kMtBlock, 7) void mt_fill(MtArgs a, F fw)
                 s[j * kMtBlock] = r[j];
             // the registers are dead from here: the compiler must read the slots back
             asm volatile("" ::: "memory");
-            mt_round(SharedUnits<F>{f, s}, a, rho);
+            mt_round_staged(f, s, a, rho);
             asm volatile("" ::: "memory");
 #pragma unroll
             for(unsigned j = 0; j < kMtSlots; j++)

@@ -146,6 +146,21 @@ static rocrand_status launch_philox(PhiloxCall a, const F& f, cudaStream_t strea
 PhiloxGenerator::PhiloxGenerator() = default;
 PhiloxGenerator::~PhiloxGenerator() = default;
 
+// Output `index` of distribution d comes from stream value index * iw / ow (index a multiple
+// of ow, output aligned to the distribution's vector), so the position is that offset.
+rocrand_status PhiloxGenerator::set_output_position(Dist d, unsigned long long index)
+{
+    if(d == Dist::U64)
+        return ROCRAND_STATUS_TYPE_ERROR;
+    DistParams p;
+    return with_functor(d, p, [&](auto f) -> rocrand_status {
+        using F = decltype(f);
+        if(index % F::ow != 0)
+            return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE;
+        return set_offset(index / F::ow * F::iw);
+    });
+}
+
 rocrand_status PhiloxGenerator::init()
 {
     if(m_initialized)

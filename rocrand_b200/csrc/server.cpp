@@ -11,6 +11,11 @@
 // handles keep their position on the host and may appear several times in one batch.
 // Each result equals the same call made alone on the handle's generator: descriptors are
 // taken in submission order from the generator's own state (batch_descriptor).
+// Requests of at least kDirectBytes run as their own ordinary call on a separate stream as
+// soon as they are admitted: at that size the call streams at the kernel's own speed, and
+// outside a batch it does not hold back the small requests it was admitted with (a batch
+// completes as a whole).  Poisson requests always go through a batch (their tables are
+// shared per lambda across streams).
 // The plain mode runs the same admission and memory pool but issues one ordinary
 // generate call per request on one stream: the per-request baseline.
 #include "admission.hpp"
@@ -113,6 +118,8 @@ public:
             if(rst != ROCRAND_STATUS_SUCCESS)
                 return rst;
         }
+        if(!m_plain && cudaStreamCreateWithFlags(&m_direct, cudaStreamNonBlocking) != cudaSuccess)
+            return ROCRAND_STATUS_INTERNAL_ERROR;
         m_worker = std::thread([this] { loop(); });
         return ROCRAND_STATUS_SUCCESS;
     }
@@ -129,9 +136,13 @@ public:
         cudaSetDevice(m_device);
         for(auto s : m_streams)
             cudaStreamSynchronize(s);
+        if(m_direct)
+            cudaStreamSynchronize(m_direct);
         m_plans.clear();
         for(auto s : m_streams)
             cudaStreamDestroy(s);
+        if(m_direct)
+            cudaStreamDestroy(m_direct);
         for(auto& h : m_handles)
             if(h.last)
                 cudaEventDestroy(h.last);
@@ -332,6 +343,22 @@ private:
         return st;
     }
 
+    // A large request as its own ordinary call on the direct stream, after its handle's
+    // previous batch or call (stateful handles); records the handle's last event.
+    rocrand_status launch_direct(Request* r)
+    {
+        Handle& h = *r->h;
+        if(h.stateful && h.last_pending)
+            cudaStreamWaitEvent(m_direct, h.last, 0);
+        const rocrand_status st = plain_call(r, m_direct);
+        if(st == ROCRAND_STATUS_SUCCESS && h.stateful)
+        {
+            cudaEventRecord(h.last, m_direct);
+            h.last_pending = true;
+        }
+        return st;
+    }
+
     void loop()
     {
         cudaSetDevice(m_device);
@@ -351,7 +378,8 @@ private:
                 }
                 for(Request* r : it->reqs)
                     finish(r, ROCRAND_STATUS_SUCCESS);
-                busy[it->stream] = false;
+                if(it->stream >= 0)
+                    busy[it->stream] = false;
                 cudaEventDestroy(it->done);
                 it      = inflight.erase(it);
                 retired = true;
@@ -386,15 +414,51 @@ private:
             {
                 std::vector<Request*> reqs;
                 admit(reqs, m_plain ? 1 : kMaxBatchRequests, m_plain ? m_budget : (size_t(8) << 30));
-                if(!reqs.empty())
+                // large requests: their own ordinary call on the direct stream
+                std::vector<Request*> direct;
+                if(!m_plain)
                 {
-                    InFlight f;
-                    f.stream = s;
+                    size_t k = 0;
+                    for(size_t i = 0; i < reqs.size(); i++)
+                    {
+                        Request* r = reqs[i];
+                        if(r->bytes >= kDirectBytes && r->dist != BD_POISSON)
+                            direct.push_back(r);
+                        else
+                            reqs[k++] = r;
+                    }
+                    reqs.resize(k);
+                }
+                if(!reqs.empty() || !direct.empty())
+                {
                     // admitted requests, their handles and the streams belong to this thread:
                     // launch without holding the queue lock, so submitters are not delayed
                     lock.unlock();
-                    rocrand_status st = launch(reqs, s);
+                    std::vector<std::pair<Request*, rocrand_status>> direct_st;
+                    for(Request* r : direct)
+                        direct_st.emplace_back(r, launch_direct(r));
+                    rocrand_status st = reqs.empty() ? ROCRAND_STATUS_SUCCESS : launch(reqs, s);
                     lock.lock();
+                    for(auto& [r, dst] : direct_st)
+                    {
+                        if(dst != ROCRAND_STATUS_SUCCESS)
+                        {
+                            finish(r, dst);
+                            continue;
+                        }
+                        InFlight f;
+                        f.stream = -1;
+                        cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
+                        cudaEventRecord(f.done, m_direct);
+                        f.reqs.push_back(r);
+                        inflight.push_back(std::move(f));
+                    }
+                    if(!direct_st.empty())
+                        m_done_cv.notify_all();
+                    if(reqs.empty())
+                        continue;
+                    InFlight f;
+                    f.stream = s;
                     if(st != ROCRAND_STATUS_SUCCESS)
                     {
                         for(Request* r : reqs)
@@ -436,6 +500,7 @@ private:
     static constexpr size_t       kPlainInFlight  = 4096;
     static constexpr size_t       kGatherRequests = 64;
     static constexpr double       kGatherGap      = 20e-6; // seconds
+    static constexpr size_t       kDirectBytes    = size_t(32) << 20;
     size_t                        m_budget;
     bool                          m_plain;
     unsigned                      m_nstreams = 1;
@@ -443,6 +508,7 @@ private:
     unsigned char*                m_pool     = nullptr;
     PoolAllocator                 m_alloc;
     std::vector<cudaStream_t>     m_streams;
+    cudaStream_t                  m_direct = nullptr; // large requests as ordinary calls
     std::vector<std::unique_ptr<BatchPlan>> m_plans;
     std::deque<Handle>            m_handles;
     AdmissionQueue<Request>       m_queue;

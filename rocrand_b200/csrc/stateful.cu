@@ -482,6 +482,20 @@ static void bases_of(Family fam, unsigned long long seed, uint4 seed4, unsigned 
     }
 }
 
+// Base states for a position reached by writing `vectors` output vectors of `values` engine
+// values each from offset 0: engine e has then stepped values * (vectors / E + (e < vectors %
+// E)) times (every vector j is served by engine j mod E), so base[0] skips values * (vectors /
+// E) and base[1] (engines below start = vectors % E) values more.
+static void bases_at_output(Family fam, unsigned long long seed, uint4 seed4, unsigned long long vectors,
+                            unsigned values, uint32_t (&base)[2][6])
+{
+    const unsigned long long q = vectors / kE;
+    seeded_state(fam, seed, seed4, base[0]);
+    host_discard(fam, base[0], q * values);
+    std::memcpy(base[1], base[0], sizeof(base[0]));
+    host_discard(fam, base[1], values);
+}
+
 StatefulBases stateful_bases(StatefulFamily fam, unsigned long long seed, unsigned long long offset)
 {
     StatefulBases b{};
@@ -602,11 +616,19 @@ public:
                 return ROCRAND_STATUS_ALLOCATION_FAILED;
             }
         }
-        m_start = static_cast<uint32_t>(m_offset % kE);
         InitArgs a{};
+        if(m_has_pos)
+        {
+            m_start = static_cast<uint32_t>(m_pos_vectors % kE);
+            bases_at_output(kFam, m_seed, m_seed4, m_pos_vectors, m_pos_values, a.base);
+        }
+        else
+        {
+            m_start = static_cast<uint32_t>(m_offset % kE);
+            bases_of(kFam, m_seed, m_seed4, m_offset, a.base);
+        }
         a.start = m_start;
         a.arena = m_arena;
-        bases_of(kFam, m_seed, m_seed4, m_offset, a.base);
         const unsigned blocks = kE / kBlock;
         if constexpr(kFam == Family::XORWOW)
         {
@@ -637,6 +659,45 @@ public:
         if(st != ROCRAND_STATUS_SUCCESS)
             return st;
         m_initialized = true;
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
+    rocrand_status set_offset(unsigned long long offset) override
+    {
+        m_has_pos = false;
+        return PseudoGeneratorBase::set_offset(offset);
+    }
+
+    // Output `index` of distribution d: vector V = index / ow was served by engine V mod E,
+    // so every engine has stepped iw * (V / E + (e < V % E)) values and the rotation starts at
+    // V mod E (xorwow.hpp:385-389 advances start by one per vector).
+    rocrand_status set_output_position(Dist d, unsigned long long index) override
+    {
+        if(d == Dist::U64)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        DistParams     p;
+        unsigned       iw = 0, ow = 1;
+        auto           body = [&](auto f) -> rocrand_status {
+            iw = decltype(f)::iw;
+            ow = decltype(f)::ow;
+            return ROCRAND_STATUS_SUCCESS;
+        };
+        rocrand_status st;
+        if constexpr(kFam == Family::MRG32K3A)
+            st = with_functor_mrg<Mrg32k3aNorm>(d, p, body);
+        else if constexpr(kFam == Family::MRG31K3P)
+            st = with_functor_mrg<Mrg31k3pNorm>(d, p, body);
+        else
+            st = with_functor(d, p, body);
+        if(st != ROCRAND_STATUS_SUCCESS)
+            return st;
+        if(index % ow != 0)
+            return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE;
+        m_offset      = 0;
+        m_has_pos     = true;
+        m_pos_vectors = index / ow;
+        m_pos_values  = iw;
+        m_initialized = false;
         return ROCRAND_STATUS_SUCCESS;
     }
 
@@ -737,6 +798,11 @@ private:
     uint4     m_seed4 = {0, 0, 0, 0};
     uint32_t* m_arena = nullptr;
     uint32_t  m_start = 0;
+    // rocrand_b200_set_output_position: engines placed after m_pos_vectors vectors of
+    // m_pos_values values each (replaces the offset until the next set_offset)
+    bool               m_has_pos     = false;
+    unsigned long long m_pos_vectors = 0;
+    unsigned           m_pos_values  = 1;
 };
 
 rocrand_generator_base_type* make_stateful(rocrand_rng_type t)

@@ -318,6 +318,37 @@ class ThreefryGenerator final : public PseudoGeneratorBase
 public:
     rocrand_rng_type type() const override { return kType; }
 
+    // Output `index` of distribution d comes from engine word index * iw / ow (index a
+    // multiple of ow, output aligned to the distribution's vector): that offset.
+    rocrand_status set_output_position(Dist d, unsigned long long index) override
+    {
+        if(sizeof(W) == 4 && d == Dist::U64)
+            return ROCRAND_STATUS_TYPE_ERROR;
+        DistParams p;
+        auto body = [&](auto f) -> rocrand_status {
+            using F = decltype(f);
+            if constexpr(D % F::iw != 0)
+                return ROCRAND_STATUS_TYPE_ERROR;
+            else
+            {
+                if(index % F::ow != 0)
+                    return ROCRAND_STATUS_LENGTH_NOT_MULTIPLE;
+                return set_offset(index / F::ow * F::iw);
+            }
+        };
+        if constexpr(sizeof(W) == 8)
+            return with_functor64(d, p, body);
+        else
+        {
+            if constexpr(D == 2)
+            {
+                if(d == Dist::NORMAL_F64 || d == Dist::LOGNORMAL_F64)
+                    return body(FnNormalD1{p.mean_d, p.std_d, false});
+            }
+            return with_functor(d, p, body);
+        }
+    }
+
     rocrand_status init() override
     {
         if(m_initialized)

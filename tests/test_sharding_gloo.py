@@ -1,14 +1,15 @@
 """Multi-GPU sharding on the CPU: two gloo ranks, each filling its slice of every stream.
 
-bench.py's multi-GPU mode gives rank r the outputs [r*n, (r+1)*n) of one stream by setting
-the generator's offset to the engine position of output r*n (bench.rank_stream); there is
-no data collective.  Here two ranks do exactly that with the oracle (the reference's
-semantics), gather their slices, and rank 0 checks that the concatenation equals one
-generator producing 2n outputs -- counter engines (Philox, ThreeFry) with one- and two-word
-distributions, stateful engines (XORWOW, MRG32k3a, LFSR113) with one-word ones.  Where no
-offset selects the slice (MT19937, MTGP32; a stateful engine consuming two values per output, whose
-offsets rotate engines by values, not outputs -- checked here too) the ranks use distinct
-seeds, and the test checks their streams differ.
+bench.py's multi-GPU mode gives rank r the outputs [r*n, (r+1)*n) of one stream by
+positioning its generator at output r*n (bench.rank_stream, rocrand_b200_set_output_position);
+there is no data collective.  The position is, by definition, the state one generator
+reaches by writing r*n outputs of that kind from offset 0.  Here two ranks reach it on the
+oracle (the reference's semantics) that way -- by a first call of r*n outputs -- gather the
+slices they write next, and rank 0 checks that the concatenation equals one generator
+producing 2n outputs: counter engines (Philox, ThreeFry) and stateful engines (XORWOW,
+MRG32k3a, LFSR113) with one- and two-value distributions.  (tests/test_output_position_gpu.py
+checks that the library's position equals that state.)  MT19937 and MTGP32 have no position:
+the ranks use distinct seeds, and the test checks their streams differ.
 """
 
 import os
@@ -24,8 +25,9 @@ import bench
 from oracle import pyorc
 
 CASES = [(404, "uniform"), (404, "uniform_double"), (410, "uint"), (410, "normal"),
-         (401, "uniform"), (402, "uniform"), (406, "uint")]
-SEEDED = [(407, "uint"), (403, "uniform"), (401, "uniform_double"), (402, "normal")]
+         (401, "uniform"), (402, "uniform"), (406, "uint"), (401, "uniform_double"), (402, "normal"),
+         (406, "normal_double")]
+SEEDED = [(407, "uint"), (403, "uniform")]
 N = 3 * 131072 + 1000  # crosses the stateful engines' slot boundary
 
 
@@ -44,11 +46,14 @@ def _rank(rank, world, port, failures):
     try:
         orc = pyorc.CLib("orc")
         for rng, d in CASES:
-            seed, off = bench.rank_stream(rng, d, rank, N)
-            assert seed == bench.SEED and off is not None
+            seed, pos = bench.rank_stream(rng, d, rank, N)
+            assert seed == bench.SEED and pos == rank * N
             params = (0.0, 1.0) if "normal" in d else ()
-            st, mine = pyorc.run_sequence(orc, rng, seed, off, [(d, N, params, 0)])[0]
-            assert st == 0
+            # the state after `pos` outputs of this kind, then this rank's slice
+            calls = ([(d, pos, params, 0)] if pos else []) + [(d, N, params, 0)]
+            res = pyorc.run_sequence(orc, rng, seed, 0, calls)
+            assert all(st == 0 for st, _ in res)
+            mine = res[-1][1]
             t = torch.from_numpy(mine.view(np.uint8).copy())
             parts = [torch.empty_like(t) for _ in range(world)]
             dist.all_gather(parts, t)
