@@ -294,10 +294,11 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
 
     def kernel_roof(i):
-        gname, _, d, _ = calls[i]
+        gname, _, d, p = calls[i]
         b = ELEM[d] * n
         gbs = b / (mean_call[i] * 1e-3) / 1e9
-        iss, iss_src = issue_bound(gname, d, n, clocks.get("sm_mhz"))
+        iss, iss_src = issue_bound(gname, d + ("" if p is None else str(list(p))), ELEM[d], n,
+                                   clocks.get("sm_mhz"))
         bound = "issue" if iss is not None and iss < peak else "hbm"
         lim = min(peak, iss) if iss is not None else peak
         return {"kernel": "%s %s%s" % (gname, d, "" if calls[i][3] is None else list(calls[i][3])),
@@ -589,15 +590,15 @@ def ref_kernels_leg(lib, calls, n, ours_ms, reps):
             "per_kernel_ms_ours_ref_ratio": per}
 
 
-def issue_bound(gname, dist, n, clock_mhz):
+def issue_bound(gname, dist_key, elem, n, clock_mhz):
     """(GB/s that the instruction issue rate allows, source) for one sweep kernel: warp
     instructions per output value from the ncu capture in NCU_INST, issued at most 4 per SM
     per clock on 148 SMs at the sampled SM clock; (None, None) where no capture exists."""
-    per_value = NCU_INST.get((gname, dist))
+    per_value = NCU_INST.get((gname, dist_key))
     if per_value is None or not clock_mhz:
         return None, None
     secs = per_value * n / (148 * 4 * clock_mhz * 1e6)
-    return ELEM[dist] * n / secs / 1e9, "%s: %.3f warp instructions per value" % (NCU_INST_SOURCE, per_value)
+    return elem * n / secs / 1e9, "%s: %.3f warp instructions per value" % (NCU_INST_SOURCE, per_value)
 
 
 # ------------------------------------------------------------------------------------

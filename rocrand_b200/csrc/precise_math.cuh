@@ -6,10 +6,12 @@
 // normal and log-normal outputs of this library are compared with them at <= 2 ulp (fp64);
 // the device's own 1-2 ulp functions can leave a 3-ulp gap after the products, so the fp64
 // transforms use these instead.  Method (standard table-driven reduction, written here):
-//  * log x: x = 2^e m with m in [sqrt(1/2), sqrt(2)); c = 1 + i/128 nearest m,
-//    r = m/c - 1 formed exactly as m*invc - 1 in double-double, then
-//    log x = e ln2 - log(invc) + r - r^2/2 + r^3 P(r) with the leading terms in
-//    double-double and one final rounding;
+//  * log x: x = 2^k z with z in [OFF, 2 OFF), OFF just above sqrt(1/2), split by integer
+//    operations on the bit pattern; the top 8 bits of z's offset pick one of 256
+//    subintervals with a tabulated invc = 1/c of at most 9 significant bits, so that
+//    r = z invc - 1 is exact in one fma (|r| < 2^-8; the subinterval around 1 has c = 1);
+//    log x = (k ln2_hi + log c_hi) + r - r^2/2 + r^3 P(r) + small terms, the first sums
+//    compensated and one final rounding;
 //  * sin/cos x (0 <= x <~ 8): x = k pi/2 + r (pi/2 in three parts), |r| = j/64 + b,
 //    sin/cos(j/64) from a double-double table, sin b and cos b - 1 by short series.
 // Both are IEEE operations only (add, mul, fma, sqrt-free), so host and device builds of
@@ -35,10 +37,10 @@ namespace pm
 {
 
 #if defined(__CUDACC__)
-static __device__ const double kLogTabDev[RB_LOG_TABLE_ROWS * 3] = RB_LOG_TABLE_INIT;
+static __device__ const double kLogTabDev[RB_LOG_ROWS * 3] = RB_LOG_INIT;
 static __device__ const double kScTabDev[RB_SC_TABLE_ROWS * 4]    = RB_SC_TABLE_INIT;
 #endif
-static const double kLogTabHost[RB_LOG_TABLE_ROWS * 3] = RB_LOG_TABLE_INIT;
+static const double kLogTabHost[RB_LOG_ROWS * 3] = RB_LOG_INIT;
 static const double kScTabHost[RB_SC_TABLE_ROWS * 4]    = RB_SC_TABLE_INIT;
 
 RB_PM_HD const double* log_table()
@@ -113,48 +115,38 @@ RB_PM_HD double log(double x)
     // The main path runs for every input (the special cases are selected at the end, so
     // that independent calls can interleave): zero, negative, NaN and infinity still give
     // a table row in range there.
-    const double   x0  = x;
-    const bool     sub = x < 0x1p-1022; // subnormal (or zero / negative: replaced below)
-    x                  = sub ? x * 0x1p54 : x;
-    int            e   = sub ? -54 : 0;
-    const uint64_t u   = bits_of(x);
-    e += static_cast<int>((u >> 52) & 0x7ff) - 1023;
-    double     m  = from_bits((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull); // [1, 2)
-    const bool up = m >= 1.4142135623730951;
-    m             = up ? m * 0.5 : m;
-    e += up ? 1 : 0;
-    const int     i   = static_cast<int>(rint((m - 1.0) * 128.0));
-    const double* row = log_table() + 3 * (i - RB_LOG_TABLE_MIN);
-    const double  invc = tab(row), lch = tab(row + 1), lcl = tab(row + 2);
-    // r = m * invc - 1 exactly, as r_hi + r_lo
-    const double ph = m * invc;
-    const double pl = fma_(m, invc, -ph);
-    double       rh, rl;
-    two_sum(ph - 1.0, pl, rh, rl); // ph - 1 is exact (ph in [0.5, 2])
-    // -r^2 / 2 as qh + ql
-    const double r2h = rh * rh;
-    const double r2l = fma_(rh, rh, -r2h) + 2.0 * rh * rl;
-    const double qh  = -0.5 * r2h;
-    const double ql  = -0.5 * r2l;
-    // r^3 (1/3 - r/4 + ... + r^6/9), |r| < 2^-7.5: the first term left out, r^10/10, is
-    // below 2^-75 of the result
-    double t = 1.0 / 9.0;
-    t        = fma_(t, rh, -1.0 / 8.0);
-    t        = fma_(t, rh, 1.0 / 7.0);
-    t        = fma_(t, rh, -1.0 / 6.0);
-    t        = fma_(t, rh, 1.0 / 5.0);
-    t        = fma_(t, rh, -1.0 / 4.0);
-    t        = fma_(t, rh, 1.0 / 3.0);
-    const double tail = t * (rh * r2h);
-    const double de   = static_cast<double>(e);
-    double       s1h, s1l, s2h, s2l, s3h, s3l;
-    // Fast two-sums: |e ln2| >= 0.69 > |log c| <= 0.35 unless e = 0; |log c| >= 2^-7 > |r|
-    // unless c = 1 (then log c = 0); |r| > r^2/2.  e * ln2_hi is exact (42-bit head).
-    fast_two_sum(de * RB_LN2_HI, lch, s1h, s1l);
-    fast_two_sum(s1h, rh, s2h, s2l);
-    fast_two_sum(s2h, qh, s3h, s3l);
-    const double low = (((s1l + s2l) + s3l) + (ql + rl)) + ((lcl + de * RB_LN2_LO) + tail);
-    const double y   = s3h + low;
+    const double x0  = x;
+    const bool   sub = x < 0x1p-1022; // subnormal (or zero / negative: replaced below)
+    x                = sub ? x * 0x1p54 : x;
+    const uint64_t ix  = bits_of(x);
+    const uint64_t tmp = ix - RB_LOG_OFF;
+    const unsigned i   = static_cast<unsigned>(tmp >> 44) & 255u;
+    const int      k   = static_cast<int>(static_cast<int64_t>(tmp) >> 52) - (sub ? 54 : 0);
+    const double   z   = from_bits(ix - (tmp & 0xfff0000000000000ull)); // x / 2^k in [OFF, 2 OFF)
+    const double*  row = log_table() + 3 * i;
+    const double   invc = tab(row), lch = tab(row + 1), lcl = tab(row + 2);
+    const double   kd   = static_cast<double>(k);
+    const double   r    = fma_(z, invc, -1.0);       // exact: |r| < 2^-8, invc has <= 9 bits
+    const double   t1   = fma_(kd, RB_LN2_HI, lch);  // exact: both multiples of 2^-42, |t1| < 2^10
+    double         s1, e1, s2, e2;
+    two_sum(t1, r, s1, e1);
+    // -r^2 / 2 = q + ql exactly
+    const double r2 = r * r;
+    const double q  = -0.5 * r2;
+    const double ql = -0.5 * fma_(r, r, -r2);
+    // |s1| >= |q|: s1 = r when t1 = 0 (the subinterval around 1), else |s1| ~ |log x| >= 2^-10
+    fast_two_sum(s1, q, s2, e2);
+    // r^3 (1/3 - r/4 + r^2/5 - r^3/6 + r^4/7 - r^5/8): the first term left out, r^9/9, is
+    // below 2^-67 of the result
+    double p = -1.0 / 8.0;
+    p        = fma_(p, r, 1.0 / 7.0);
+    p        = fma_(p, r, -1.0 / 6.0);
+    p        = fma_(p, r, 1.0 / 5.0);
+    p        = fma_(p, r, -1.0 / 4.0);
+    p        = fma_(p, r, 1.0 / 3.0);
+    const double tail = p * (r2 * r);
+    const double low  = ((e1 + e2) + (ql + lcl)) + fma_(kd, RB_LN2_LO, tail);
+    const double y    = s2 + low;
     return x0 > 0.0 ? (x0 == INFINITY ? x0 : y) : (x0 == 0.0 ? -INFINITY : NAN);
 }
 
