@@ -557,12 +557,13 @@ def ref_kernels_leg(lib, calls, n, ours_ms, reps):
             compared += 1
             same += int(torch.equal(a[:nb], b[:nb]))
         elif d in ("normal", "normal_double"):
-            # distance of the reference kernel's normals from ours (ours are within the stated
-            # ulp bound of the reference's host generator), in ulps of the output
-            it = torch.int32 if d == "normal" else torch.int64
+            # share of the reference kernel's normals farther than the host-parity bound (4 ulp
+            # fp32, 2 ulp fp64) from ours, which are within it of the reference's host output:
+            # the reference's kernels use the fast __sincosf / sincospi device functions
+            it, tol = (torch.int32, 4) if d == "normal" else (torch.int64, 2)
             x, y = a[:nb].view(it), b[:nb].view(it)
-            same_sign = (x >= 0) == (y >= 0)
-            ulps["%s %s" % (gname, d)] = int((x - y).abs()[same_sign].max().item())
+            far = ((x >= 0) != (y >= 0)) | ((x - y).abs() > tol)
+            ulps["%s %s" % (gname, d)] = round(float(far.sum().item()) / (nb // (4 if d == "normal" else 8)), 6)
         ms = []
         for (L, g), (fn, buf) in zip(gens, fns):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -586,7 +587,7 @@ def ref_kernels_leg(lib, calls, n, ours_ms, reps):
             "speedup": round(ref_tot / ours_tot, 2),
             "min_kernel_speedup": ratios[0], "median_kernel_speedup": ratios[len(ratios) // 2],
             "identical_bit_exact_outputs": "%d of %d" % (same, compared),
-            "ref_normal_max_ulps_from_ours": ulps,
+            "ref_normals_outside_host_bound": ulps,
             "per_kernel_ms_ours_ref_ratio": per}
 
 

@@ -9,8 +9,8 @@
 // logf (glibc) is not correctly rounded: on the ~11.6 million distinct arguments this
 // formula can produce, 0.93 % of its results are the other neighbour of the exact value.
 //
-// Method.  The device evaluates an accurate logarithm L (precise_math.cuh, double
-// precision) and rounds it to float, f.  The host's result differs from f only where the
+// Method.  The device evaluates a logarithm L to about one double ulp (precise_math.cuh
+// log_unit) and rounds it to float, f.  The host's result differs from f only where the
 // exact value lies close to the midpoint between f and its neighbour on the side of L.  The
 // build (rocrand_b200/data/make_logf_replay.cpp) runs the host's logf over every argument
 // the formula can reach and records
@@ -76,7 +76,7 @@ RB_PM_HD float step(float f, bool up)
 // (0 .. 32768; larger = safer).  t must be finite and positive.
 RB_PM_HD float base(float t, double& dist)
 {
-    const double L  = pm::log(static_cast<double>(t));
+    const double L  = pm::log_unit(static_cast<double>(t));
     const float  f  = static_cast<float>(L);
     const double fd = static_cast<double>(f);
     const float  nb = step(f, L > fd);

@@ -14,8 +14,10 @@
 // Requests of at least kDirectBytes run as their own ordinary call on a separate stream as
 // soon as they are admitted: at that size the call streams at the kernel's own speed, and
 // outside a batch it does not hold back the small requests it was admitted with (a batch
-// completes as a whole).  Poisson requests always go through a batch (their tables are
-// shared per lambda across streams).
+// completes as a whole).  A request that finds no other queued runs alone as an ordinary
+// call on a third stream, so batching costs a lone request no waiting.  Poisson requests go
+// through batches (whose tables are shared per lambda across streams) or, alone, through
+// the single-request stream.
 // The plain mode runs the same admission and memory pool but issues one ordinary
 // generate call per request on one stream: the per-request baseline.
 #include "admission.hpp"
@@ -118,7 +120,9 @@ public:
             if(rst != ROCRAND_STATUS_SUCCESS)
                 return rst;
         }
-        if(!m_plain && cudaStreamCreateWithFlags(&m_direct, cudaStreamNonBlocking) != cudaSuccess)
+        if(!m_plain
+           && (cudaStreamCreateWithFlags(&m_direct, cudaStreamNonBlocking) != cudaSuccess
+               || cudaStreamCreateWithFlags(&m_single, cudaStreamNonBlocking) != cudaSuccess))
             return ROCRAND_STATUS_INTERNAL_ERROR;
         m_worker = std::thread([this] { loop(); });
         return ROCRAND_STATUS_SUCCESS;
@@ -138,11 +142,15 @@ public:
             cudaStreamSynchronize(s);
         if(m_direct)
             cudaStreamSynchronize(m_direct);
+        if(m_single)
+            cudaStreamSynchronize(m_single);
         m_plans.clear();
         for(auto s : m_streams)
             cudaStreamDestroy(s);
         if(m_direct)
             cudaStreamDestroy(m_direct);
+        if(m_single)
+            cudaStreamDestroy(m_single);
         for(auto& h : m_handles)
             if(h.last)
                 cudaEventDestroy(h.last);
@@ -214,7 +222,6 @@ public:
         ticket               = r->ticket;
         m_queue.push(r.get(), handle);
         m_reqs[ticket] = std::move(r);
-        m_last_submit  = now_s();
         m_cv.notify_all();
         return ROCRAND_STATUS_SUCCESS;
     }
@@ -308,16 +315,6 @@ private:
     rocrand_status launch(std::vector<Request*>& reqs, int s)
     {
         cudaStream_t stream = m_streams[s];
-        if(!m_plain && reqs.size() == 1 && reqs[0]->dist != BD_POISSON)
-        {
-            // a batch of one: the ordinary call is the shorter launch.  (Poisson stays on the
-            // batch path, whose tables are shared across streams; a generator's own table
-            // would be refreshed on this stream while another stream may still read it.)
-            Handle& h = *reqs[0]->h;
-            if(h.stateful && h.last_pending)
-                cudaStreamWaitEvent(stream, h.last, 0);
-            return plain_call(reqs[0], stream);
-        }
         if(m_plain)
         {
             return plain_call(reqs[0], stream);
@@ -343,17 +340,19 @@ private:
         return st;
     }
 
-    // A large request as its own ordinary call on the direct stream, after its handle's
-    // previous batch or call (stateful handles); records the handle's last event.
-    rocrand_status launch_direct(Request* r)
+    // A request as its own ordinary call on `stream` (the direct or the single-request
+    // stream), after its handle's previous batch or call (stateful handles); records the
+    // handle's last event.  Poisson requests come here only on the single-request stream,
+    // so a generator's own Poisson table is only ever refreshed and read there.
+    rocrand_status launch_alone(Request* r, cudaStream_t stream)
     {
         Handle& h = *r->h;
         if(h.stateful && h.last_pending)
-            cudaStreamWaitEvent(m_direct, h.last, 0);
-        const rocrand_status st = plain_call(r, m_direct);
+            cudaStreamWaitEvent(stream, h.last, 0);
+        const rocrand_status st = plain_call(r, stream);
         if(st == ROCRAND_STATUS_SUCCESS && h.stateful)
         {
-            cudaEventRecord(h.last, m_direct);
+            cudaEventRecord(h.last, stream);
             h.last_pending = true;
         }
         return st;
@@ -380,6 +379,8 @@ private:
                     finish(r, ROCRAND_STATUS_SUCCESS);
                 if(it->stream >= 0)
                     busy[it->stream] = false;
+                else if(it->stream == kSingleStream)
+                    m_singles--;
                 cudaEventDestroy(it->done);
                 it      = inflight.erase(it);
                 retired = true;
@@ -393,29 +394,36 @@ private:
             }
             if(m_stop && m_queue.empty() && inflight.empty())
                 return;
-            // start a batch on a free stream (plain calls: one stream, queued back to back)
-            int s = -1;
+            // What to start:
+            //  * plain mode: one ordinary call per request on stream 0, queued back to back;
+            //  * otherwise, with two or more requests queued and a batch stream free: a batch
+            //    of what admission takes; with one queued (or every batch stream busy): that
+            //    request alone as an ordinary call on the single-request stream, so a lone
+            //    request waits neither for others to gather nor for a batch stream.
+            //  In both, admitted requests of at least kDirectBytes run as ordinary calls on
+            //  the direct stream.
+            int  s     = -1;
+            bool batch = false;
             if(m_plain)
                 s = inflight.size() < kPlainInFlight ? 0 : -1;
             else
+            {
                 for(unsigned k = 0; k < m_nstreams; k++)
                     if(!busy[k])
                     {
                         s = static_cast<int>(k);
                         break;
                     }
-            // While a burst of submissions is arriving and a batch is already on the device,
-            // let a few more requests gather instead of launching tiny batches back to back
-            // (each launch costs its own descriptor upload): hold while fewer than
-            // kGatherRequests are queued and the last submission was under kGatherGap ago.
-            const bool gather = !m_plain && !inflight.empty() && m_queue.size() < kGatherRequests
-                                && now_s() - m_last_submit < kGatherGap;
-            if(s >= 0 && !m_queue.empty() && !gather)
+                batch = s >= 0 && m_queue.size() >= 2;
+            }
+            const bool single = !m_plain && !batch && m_singles < kPlainInFlight;
+            if(!m_queue.empty() && (m_plain ? s >= 0 : (batch || single)))
             {
                 std::vector<Request*> reqs;
-                admit(reqs, m_plain ? 1 : kMaxBatchRequests, m_plain ? m_budget : (size_t(8) << 30));
-                // large requests: their own ordinary call on the direct stream
-                std::vector<Request*> direct;
+                admit(reqs, batch ? kMaxBatchRequests : 1, m_plain ? m_budget : (size_t(8) << 30));
+                // large requests: their own ordinary call on the direct stream; a batch that
+                // keeps one request runs it as a single
+                std::vector<Request*> direct, singles;
                 if(!m_plain)
                 {
                     size_t k = 0;
@@ -428,32 +436,44 @@ private:
                             reqs[k++] = r;
                     }
                     reqs.resize(k);
+                    if(reqs.size() == 1)
+                    {
+                        singles.push_back(reqs[0]);
+                        reqs.clear();
+                    }
                 }
-                if(!reqs.empty() || !direct.empty())
+                if(!reqs.empty() || !direct.empty() || !singles.empty())
                 {
                     // admitted requests, their handles and the streams belong to this thread:
                     // launch without holding the queue lock, so submitters are not delayed
                     lock.unlock();
-                    std::vector<std::pair<Request*, rocrand_status>> direct_st;
+                    std::vector<std::pair<Request*, rocrand_status>> own_st;
                     for(Request* r : direct)
-                        direct_st.emplace_back(r, launch_direct(r));
+                        own_st.emplace_back(r, launch_alone(r, m_direct));
+                    const size_t n_direct = own_st.size();
+                    for(Request* r : singles)
+                        own_st.emplace_back(r, launch_alone(r, m_single));
                     rocrand_status st = reqs.empty() ? ROCRAND_STATUS_SUCCESS : launch(reqs, s);
                     lock.lock();
-                    for(auto& [r, dst] : direct_st)
+                    for(size_t i = 0; i < own_st.size(); i++)
                     {
-                        if(dst != ROCRAND_STATUS_SUCCESS)
+                        Request* const       r   = own_st[i].first;
+                        const rocrand_status rst = own_st[i].second;
+                        if(rst != ROCRAND_STATUS_SUCCESS)
                         {
-                            finish(r, dst);
+                            finish(r, rst);
                             continue;
                         }
                         InFlight f;
-                        f.stream = -1;
+                        f.stream = i < n_direct ? kDirectStream : kSingleStream;
                         cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
-                        cudaEventRecord(f.done, m_direct);
+                        cudaEventRecord(f.done, i < n_direct ? m_direct : m_single);
                         f.reqs.push_back(r);
+                        if(i >= n_direct)
+                            m_singles++;
                         inflight.push_back(std::move(f));
                     }
-                    if(!direct_st.empty())
+                    if(!own_st.empty())
                         m_done_cv.notify_all();
                     if(reqs.empty())
                         continue;
@@ -498,9 +518,9 @@ private:
 
     static constexpr size_t       kMaxBatchRequests = 8192;
     static constexpr size_t       kPlainInFlight  = 4096;
-    static constexpr size_t       kGatherRequests = 64;
-    static constexpr double       kGatherGap      = 20e-6; // seconds
     static constexpr size_t       kDirectBytes    = size_t(32) << 20;
+    static constexpr int          kDirectStream   = -1; // InFlight::stream of a direct call
+    static constexpr int          kSingleStream   = -2; // ... and of a single request
     size_t                        m_budget;
     bool                          m_plain;
     unsigned                      m_nstreams = 1;
@@ -509,6 +529,8 @@ private:
     PoolAllocator                 m_alloc;
     std::vector<cudaStream_t>     m_streams;
     cudaStream_t                  m_direct = nullptr; // large requests as ordinary calls
+    cudaStream_t                  m_single = nullptr; // lone requests as ordinary calls
+    size_t                        m_singles = 0;      // single-request calls in flight
     std::vector<std::unique_ptr<BatchPlan>> m_plans;
     std::deque<Handle>            m_handles;
     AdmissionQueue<Request>       m_queue;
@@ -518,7 +540,6 @@ private:
     std::condition_variable       m_cv, m_done_cv;
     std::thread                   m_worker;
     bool                          m_stop        = false;
-    double                        m_last_submit = 0.0;
 };
 
 } // namespace rb200

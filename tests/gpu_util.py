@@ -24,6 +24,7 @@ def bit_exact(rng, dist):
 # Elements of fp64 outputs that are outside the forward ulp bound and were accepted by the
 # backward-error rule of compare_call, per (rng, dist): [accepted elements, elements compared].
 FP64_EXCEPTIONS = {}
+FP64_EXCEPTION_RATE = 1e-4
 
 # ulp tolerances of the floating-point distributions against the host oracle (glibc libm).
 # They bound the error of the deviate the library computes, stddev * N, in ulps of that
@@ -212,4 +213,7 @@ def compare_call(orc, rng, seed, offset, dims, calls, k, got, exp):
     acc = FP64_EXCEPTIONS.setdefault((rng, dist), [0, 0])
     acc[0] += outside
     acc[1] += int(exp.size)
+    # the stated rate of such elements: at most FP64_EXCEPTION_RATE of a call (measured:
+    # about 4e-6 for Box-Muller, 2e-5 to 4e-5 for the inverse-erf normal)
+    assert outside <= max(2, FP64_EXCEPTION_RATE * exp.size), (rng, dist, outside, exp.size)
     return worst

@@ -7,6 +7,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <random>
 
@@ -52,7 +53,34 @@ int main(int argc, char** argv)
         miss_cos += c != static_cast<double>(ec);
         miss_gsin += std::sin(ang) != static_cast<double>(es);
     }
+    // log near 1 (where the result is small and the reduction must not cancel) and at both
+    // sides of every table boundary, in three binades
+    double max_near = 0;
+    long   miss_near = 0, n_near = 0;
+    auto   near = [&](double x) {
+        const __float128 lx = logq((__float128)x);
+        const double     a  = rb200::pm::log(x);
+        max_near            = std::fmax(max_near, std::fabs(ulp_err(a, lx)));
+        miss_near += a != static_cast<double>(lx);
+        n_near++;
+    };
+    for(long k = 1; k <= 200000; k++)
+    {
+        near(1.0 + static_cast<double>(k) * 0x1p-52);
+        near(1.0 - static_cast<double>(k) * 0x1p-53);
+    }
+    for(uint64_t i = 0; i < RB_LOG_ROWS; i++)
+        for(int d = -3; d <= 3; d++)
+        {
+            double z;
+            const uint64_t b = RB_LOG_OFF + (i << 44) + static_cast<uint64_t>(static_cast<int64_t>(d));
+            std::memcpy(&z, &b, 8);
+            near(z);
+            near(z * 0.5);
+            near(z * 1024.0);
+        }
     std::printf("log %.6f %ld %ld\n", max_log, miss_log, n);
+    std::printf("log_near %.6f %ld %ld\n", max_near, miss_near, n_near);
     std::printf("sin %.6f %ld %ld\n", max_sin, miss_sin, n);
     std::printf("cos %.6f %ld %ld\n", max_cos, miss_cos, n);
     std::printf("logf 0 %ld %ld\n", miss_logf, n);

@@ -39,7 +39,7 @@ def report(tmp_path_factory):
 
 
 def test_log_sin_cos_nearly_correctly_rounded(report):
-    for name, allowed in (("log", 3), ("sin", 30), ("cos", 30), ("logf", 3)):
+    for name, allowed in (("log", 3), ("log_near", 3), ("sin", 30), ("cos", 30), ("logf", 3)):
         err, miss, n = report[name][0]
         assert float(err) <= 0.5 + 2.0 ** -10, (name, err)
         assert int(miss) <= allowed, (name, miss, n)
