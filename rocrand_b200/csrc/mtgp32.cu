@@ -95,26 +95,33 @@ __global__ void __launch_bounds__(kMtgpBlock) mtgp_fill(MtgpArgs a, F fw)
     constexpr unsigned ow        = F::ow;
     constexpr unsigned VB        = ow * sizeof(T);
     const unsigned long long str = static_cast<unsigned long long>(kMtgpGens) * kMtgpBlock;
-    const unsigned long long i0  = static_cast<unsigned long long>(b) * kMtgpBlock + t;
-    // Units of this thread: full vectors while index < vec_n_down, one more while index <
-    // vec_n_up (stored if index < vec_n), then the head/tail unit of a misaligned call.
-    // vec_n_down and vec_n_up are multiples of 256, so the counts are the same for every
-    // thread of the block and every thread takes every step.
-    const unsigned long long u_full = i0 < a.vec_n_down ? (a.vec_n_down - i0 + str - 1) / str : 0;
-    const unsigned long long u_part = i0 + u_full * str < a.vec_n_up ? 1 : 0;
-    const unsigned long long u_all
-        = u_full + u_part + ((ow > 1 && (a.head > 0 || a.tail > 0)) ? 1 : 0);
-    auto emit = [&](unsigned long long u, const uint32_t (&in)[F::iw]) {
-        T out[ow];
+    unsigned long long index     = static_cast<unsigned long long>(b) * kMtgpBlock + t;
+    uint32_t           in[F::iw];
+    T                  out[ow];
+    auto               gen = [&]() {
+#pragma unroll
+        for(unsigned i = 0; i < F::iw; i++)
+            in[i] = step();
         f(in, out);
-        const unsigned long long index = i0 + u * str;
-        if(u < u_full || (u < u_full + u_part && index < a.vec_n))
-        {
+    };
+    // index < vec_n_down and index < vec_n_up are the same in the whole block (both are
+    // multiples of 256), so every thread takes every step
+    while(index < a.vec_n_down)
+    {
+        gen();
+        store_small(a.vec + index * VB, out);
+        index += str;
+    }
+    if(index < a.vec_n_up)
+    {
+        gen();
+        if(index < a.vec_n)
             store_small(a.vec + index * VB, out);
-            return;
-        }
-        if(u < u_full + u_part)
-            return;
+        index += str;
+    }
+    if(ow > 1 && (a.head > 0 || a.tail > 0))
+    {
+        gen();
         T* data = reinterpret_cast<T*>(a.data);
         if(index == a.vec_n_up)
             for(unsigned o = 0; o < a.head; o++)
@@ -122,28 +129,6 @@ __global__ void __launch_bounds__(kMtgpBlock) mtgp_fill(MtgpArgs a, F fw)
         if(index == a.vec_n_up + 1)
             for(unsigned o = 0; o < a.tail; o++)
                 data[a.n - a.tail + o] = out[o];
-    };
-    // Software pipeline: the values of unit u + 1 are stepped before unit u is transformed
-    // and stored, so the transform (a table lookup for Poisson, Box-Muller for normals)
-    // overlaps the next step instead of lengthening the chain of dependent block steps.
-    if(u_all > 0)
-    {
-        uint32_t cur[F::iw];
-#pragma unroll
-        for(unsigned i = 0; i < F::iw; i++)
-            cur[i] = step();
-        for(unsigned long long u = 1; u < u_all; u++)
-        {
-            uint32_t nxt[F::iw];
-#pragma unroll
-            for(unsigned i = 0; i < F::iw; i++)
-                nxt[i] = step();
-            emit(u - 1, cur);
-#pragma unroll
-            for(unsigned i = 0; i < F::iw; i++)
-                cur[i] = nxt[i];
-        }
-        emit(u_all - 1, cur);
     }
     for(int i = t; i < kMtgpState; i += kMtgpBlock)
         a.rings[b * kMtgpState + i] = s[i];
