@@ -440,7 +440,7 @@ def run_ours(args):
     print(json.dumps(line))
 
 
-def quasi_leg(lib, reps):
+def quasi_leg(lib, reps, only=""):
     """The quasi-random workload: Sobol32 and scrambled Sobol64, 1 / 64 / 1000 dimensions x
     2^20 points per dimension at offset 4096, uniform fp64 and normal fp32, dimension-major.
     Each case: one generator, 2 untimed calls, then `reps` calls timed with CUDA events on
@@ -453,6 +453,8 @@ def quasi_leg(lib, reps):
     for gname, gtype in QUASI_GENERATORS:
         for dims in QUASI_DIMS:
             for d, p in QUASI_DISTS:
+                if only and only != "%s:%s:%d" % (gname, d, dims):
+                    continue
                 g = c_void_p()
                 rb.check_rocrand(lib.rocrand_create_generator(ctypes.byref(g), gtype))
                 rb.check_rocrand(lib.rocrand_set_quasi_random_generator_dimensions(g, dims))
@@ -483,7 +485,7 @@ def quasi_leg(lib, reps):
                 tot_b += b
                 tot_ms += ms
     del out
-    return {"gbs": round(tot_b / (tot_ms * 1e-3) / 1e9, 1), "cases": res,
+    return {"gbs": round(tot_b / (tot_ms * 1e-3) / 1e9, 1) if tot_ms else None, "cases": res,
             "workload": "2^20 points/dim, offset 4096, %d calls each" % reps}
 
 
@@ -963,6 +965,8 @@ def main():
     ap.add_argument("--only", default="", help="gen:dist[:param],... subset of the sweep")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-fill and serving legs")
     ap.add_argument("--no-quasi", action="store_true", help="skip the quasi-random (Sobol) leg")
+    ap.add_argument("--quasi-only", action="store_true",
+                    help="only the quasi-random leg (--only sobol32:normal:64 picks one case), --steps calls each")
     ap.add_argument("--no-ref-kernels", action="store_true",
                     help="skip timing the reference's own device kernels (oracle/_ref gpu build)")
     ap.add_argument("--sweep-only", action="store_true",
@@ -972,6 +976,13 @@ def main():
     ap.add_argument("--quick-batched", action="store_true",
                     help="batched-fill leg on 1024 + 1024 generators instead of 4096 + 4096")
     args = ap.parse_args()
+    if args.quasi_only:
+        # the quasi-random leg alone (one case with --only gen:dist:dims), for profiling
+        import torch
+        import rocrand_b200 as rb
+        torch.cuda.set_device(0)
+        print(json.dumps(quasi_leg(rb.load_library(), args.steps, args.only)))
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
