@@ -67,7 +67,118 @@ NCU_TRAFFIC = {
 # ncu capture of the sweep at n = 2^24 (profiles/sweep_instructions_n2p24.md); the issue bound
 # of a kernel is these instructions at 4 per SM per clock.  Filled from that capture.
 NCU_INST_SOURCE = "profiles/sweep_instructions_n2p24.md"
-NCU_INST = {}
+NCU_INST = {
+    ("philox4x32_10", "uint"): 0.3647,
+    ("philox4x32_10", "uniform"): 0.4155,
+    ("philox4x32_10", "uniform_double"): 0.8292,
+    ("philox4x32_10", "uniform_half"): 0.2744,
+    ("philox4x32_10", "normal[0.0, 1.0]"): 1.6415,
+    ("philox4x32_10", "normal_double[0.0, 1.0]"): 4.2726,
+    ("philox4x32_10", "log_normal[0.0, 1.0]"): 1.9227,
+    ("philox4x32_10", "poisson[0.5]"): 0.6473,
+    ("philox4x32_10", "poisson[10.0]"): 0.6482,
+    ("philox4x32_10", "poisson[1000.0]"): 0.6567,
+    ("xorwow", "uint"): 0.3291,
+    ("xorwow", "uniform"): 0.3970,
+    ("xorwow", "uniform_double"): 0.6548,
+    ("xorwow", "uniform_half"): 0.2766,
+    ("xorwow", "normal[0.0, 1.0]"): 1.5476,
+    ("xorwow", "normal_double[0.0, 1.0]"): 4.0022,
+    ("xorwow", "log_normal[0.0, 1.0]"): 1.8289,
+    ("xorwow", "poisson[0.5]"): 0.6151,
+    ("xorwow", "poisson[10.0]"): 0.6155,
+    ("xorwow", "poisson[1000.0]"): 0.6190,
+    ("mrg32k3a", "uint"): 1.3374,
+    ("mrg32k3a", "uniform"): 1.3062,
+    ("mrg32k3a", "uniform_double"): 1.2749,
+    ("mrg32k3a", "uniform_half"): 0.7664,
+    ("mrg32k3a", "normal[0.0, 1.0]"): 2.4937,
+    ("mrg32k3a", "normal_double[0.0, 1.0]"): 4.7173,
+    ("mrg32k3a", "log_normal[0.0, 1.0]"): 2.7749,
+    ("mrg32k3a", "poisson[0.5]"): 1.6234,
+    ("mrg32k3a", "poisson[10.0]"): 1.6238,
+    ("mrg32k3a", "poisson[1000.0]"): 1.6273,
+    ("lfsr113", "uint"): 0.9768,
+    ("lfsr113", "uniform"): 1.0706,
+    ("lfsr113", "uniform_double"): 1.7893,
+    ("lfsr113", "uniform_half"): 0.6060,
+    ("lfsr113", "normal[0.0, 1.0]"): 2.0898,
+    ("lfsr113", "normal_double[0.0, 1.0]"): 5.0002,
+    ("lfsr113", "log_normal[0.0, 1.0]"): 2.3711,
+    ("lfsr113", "poisson[0.5]"): 1.2609,
+    ("lfsr113", "poisson[10.0]"): 1.2613,
+    ("lfsr113", "poisson[1000.0]"): 1.2647,
+    ("mt19937", "uint"): 0.8396,
+    ("mt19937", "uniform"): 0.9146,
+    ("mt19937", "uniform_double"): 1.3757,
+    ("mt19937", "uniform_half"): 0.6749,
+    ("mt19937", "normal[0.0, 1.0]"): 2.3196,
+    ("mt19937", "normal_double[0.0, 1.0]"): 5.2681,
+    ("mt19937", "log_normal[0.0, 1.0]"): 2.6008,
+    ("mt19937", "poisson[0.5]"): 1.1601,
+    ("mt19937", "poisson[10.0]"): 1.1608,
+    ("mt19937", "poisson[1000.0]"): 1.1660,
+    ("threefry4x32_20", "uint"): 1.1911,
+    ("threefry4x32_20", "uniform"): 1.2614,
+    ("threefry4x32_20", "uniform_double"): 2.5036,
+    ("threefry4x32_20", "uniform_half"): 0.6872,
+    ("threefry4x32_20", "normal[0.0, 1.0]"): 2.4985,
+    ("threefry4x32_20", "normal_double[0.0, 1.0]"): 5.8746,
+    ("threefry4x32_20", "log_normal[0.0, 1.0]"): 2.7797,
+    ("threefry4x32_20", "poisson[0.5]"): 1.4929,
+    ("threefry4x32_20", "poisson[10.0]"): 1.4938,
+    ("threefry4x32_20", "poisson[1000.0]"): 1.5023,
+    ("mtgp32", "uint"): 1.1285,
+    ("mtgp32", "uniform"): 1.1989,
+    ("mtgp32", "uniform_double"): 2.9434,
+    ("mtgp32", "uniform_half"): 0.8387,
+    ("mtgp32", "normal[0.0, 1.0]"): 2.9242,
+    ("mtgp32", "normal_double[0.0, 1.0]"): 5.9064,
+    ("mtgp32", "log_normal[0.0, 1.0]"): 3.2054,
+    ("mtgp32", "poisson[0.5]"): 1.7156,
+    ("mtgp32", "poisson[10.0]"): 1.7160,
+    ("mtgp32", "poisson[1000.0]"): 1.7199,
+    ("mrg31k3p", "uint"): 1.5664,
+    ("mrg31k3p", "uniform"): 1.5352,
+    ("mrg31k3p", "uniform_double"): 1.5029,
+    ("mrg31k3p", "uniform_half"): 0.8962,
+    ("mrg31k3p", "normal[0.0, 1.0]"): 2.6921,
+    ("mrg31k3p", "normal_double[0.0, 1.0]"): 4.8748,
+    ("mrg31k3p", "log_normal[0.0, 1.0]"): 2.9734,
+    ("mrg31k3p", "poisson[0.5]"): 1.8515,
+    ("mrg31k3p", "poisson[10.0]"): 1.8518,
+    ("mrg31k3p", "poisson[1000.0]"): 1.8553,
+    ("threefry2x32_20", "uint"): 1.2033,
+    ("threefry2x32_20", "uniform"): 1.2814,
+    ("threefry2x32_20", "uniform_double"): 2.5471,
+    ("threefry2x32_20", "uniform_half"): 0.6955,
+    ("threefry2x32_20", "normal[0.0, 1.0]"): 2.6073,
+    ("threefry2x32_20", "normal_double[0.0, 1.0]"): 5.9723,
+    ("threefry2x32_20", "log_normal[0.0, 1.0]"): 2.8886,
+    ("threefry2x32_20", "poisson[0.5]"): 1.4889,
+    ("threefry2x32_20", "poisson[10.0]"): 1.4899,
+    ("threefry2x32_20", "poisson[1000.0]"): 1.4983,
+    ("threefry2x64_20", "uint"): 1.2759,
+    ("threefry2x64_20", "uniform"): 2.6118,
+    ("threefry2x64_20", "uniform_double"): 2.6899,
+    ("threefry2x64_20", "uniform_half"): 0.7368,
+    ("threefry2x64_20", "normal[0.0, 1.0]"): 2.6313,
+    ("threefry2x64_20", "normal_double[0.0, 1.0]"): 6.2311,
+    ("threefry2x64_20", "log_normal[0.0, 1.0]"): 2.9126,
+    ("threefry2x64_20", "poisson[0.5]"): 2.9953,
+    ("threefry2x64_20", "poisson[10.0]"): 2.9963,
+    ("threefry2x64_20", "poisson[1000.0]"): 3.0074,
+    ("threefry4x64_20", "uint"): 1.2798,
+    ("threefry4x64_20", "uniform"): 2.6001,
+    ("threefry4x64_20", "uniform_double"): 2.6783,
+    ("threefry4x64_20", "uniform_half"): 0.7388,
+    ("threefry4x64_20", "normal[0.0, 1.0]"): 2.6241,
+    ("threefry4x64_20", "normal_double[0.0, 1.0]"): 6.1945,
+    ("threefry4x64_20", "log_normal[0.0, 1.0]"): 2.9053,
+    ("threefry4x64_20", "poisson[0.5]"): 3.0316,
+    ("threefry4x64_20", "poisson[10.0]"): 3.0327,
+    ("threefry4x64_20", "poisson[1000.0]"): 3.0437,
+}
 
 
 def ncu_traffic(gname, dist, out_bytes):
@@ -920,13 +1031,16 @@ def run_reference(args):
         return
     calls = select_calls(args.only)
     threads = os.cpu_count() or 1
+    # each step a bounded sample of the sweep (2^22 values per call, 1/64 of the GPU's 2^28),
+    # so that the default 20 + 5 steps end within a few minutes
+    step_n = max(1 << 16, args.cpu_n // 4)
     for _ in range(args.warmup):
-        cpu_sample(args.cpu_n // 4, calls, threads)
+        cpu_sample(step_n // 4, calls, threads)
     nb = 0
     secs = 0.0
     kind = None
     for _ in range(args.steps):
-        b, s, kind = cpu_sample(args.cpu_n, calls, threads)
+        b, s, kind = cpu_sample(step_n, calls, threads)
         nb += b
         secs += s
     value = nb / secs / 1e9
@@ -945,9 +1059,9 @@ def run_reference(args):
         "dtype": "u32/f32/f64/f16 outputs, int32 engine arithmetic",
         "data": "synthetic: seeded generator streams (seed 0xdeadbeef), no input data",
         "config": {"workload": "plain single-generator sweep, n=2^28 values per call (sampled)",
-                   "generators": [g for g, _ in SWEEP_GENERATORS], "n_per_call_sampled": args.cpu_n},
+                   "families": ",".join(g for g, _ in SWEEP_GENERATORS), "n_per_call_sampled": step_n},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-                         "sample": "n=%d values per call per step, %d threads" % (args.cpu_n, threads)},
+                         "sample": "n=%d values per call per step, %d threads" % (step_n, threads)},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

@@ -84,7 +84,10 @@ RB_PM_HD float base(float t, double& dist)
     const double mid = 0.5 * (fd + nd);                 // exact
     const double ulp = nd > fd ? nd - fd : fd - nd;     // exact, a power of two
     const double gap = L > mid ? L - mid : mid - L;
-    dist             = gap / ulp * 65536.0;             // division by a power of two: exact
+    // 2^16 / ulp built from ulp's exponent (an exact power of two, no division)
+    const uint64_t e     = (pm::bits_of(ulp) >> 52) & 0x7ff;
+    const double   scale = pm::from_bits((2046ull + 16ull - e) << 52);
+    dist                 = gap * scale;
     return f;
 }
 
