@@ -949,12 +949,18 @@ def _ref_lib():
 _SEEDED = {}  # MT19937 / MTGP32 host streams, seeded once per process
 
 
+_SEEDED = {}  # host generators per (call, threads, size): created, seeded and warmed once
+
+
 def cpu_sample(n_per_call, calls, threads):
     """Runs every call of the sweep on the reference's host generators, n_per_call values
-    each, split over `threads` host threads (each its own generator, offset to its slice).
-    MT19937 and MTGP32 have no offset, so each thread runs its own seed (seeded and warmed
-    untimed); because the reference's host MT19937 spends minutes seeding its 8192
-    generators, those are the C port's.  Returns (bytes, seconds, kind)."""
+    each, split over `threads` host threads, each its own generator on its own slice of the
+    stream (an offset slice; MT19937 and MTGP32, which have no offset, a seed of their own).
+    The generators are created, seeded and run once untimed the first time a call is sampled
+    (the host generators seed their 131072 or 8192 engines on the first call), and later
+    samples continue their streams, so the timed region is steady-state generation, as on the
+    GPU.  The reference's host MT19937 spends minutes seeding its 8192 generators, so those
+    are the C port's.  Returns (bytes, seconds, kind)."""
     import numpy as np
     from concurrent.futures import ThreadPoolExecutor
     from oracle import pyorc
@@ -971,10 +977,13 @@ def cpu_sample(n_per_call, calls, threads):
         bounds = [(i * chunk, (i + 1) * chunk if i < threads - 1 else n_per_call) for i in range(threads)]
         fn = lib.fn(suffix)
         args = pyorc.dist_args(d, p if p is not None else ())
-        key = (gtype, d, p, threads)
-        if gtype in NO_OFFSET and key in _SEEDED:
-            gens = _SEEDED[key]
-        else:
+        key = (gtype, threads, n_per_call)  # one set of generators per family
+
+        def work(i, gens, out):
+            a, b = bounds[i]
+            return fn(gens[i], c_void_p(out[a:b].ctypes.data), c_size_t(b - a), *args)
+
+        if key not in _SEEDED:
             gens = []
             for i, (a, b) in enumerate(bounds):
                 g = lib.create(gtype)
@@ -982,33 +991,17 @@ def cpu_sample(n_per_call, calls, threads):
                     lib.set_seed(g, SEED + i)
                 else:
                     lib.set_seed(g, SEED)
-                    lib.set_offset(g, stream_offset(d, a))
+                    lib.set_offset(g, a)
                 gens.append(g)
-        if gtype in NO_OFFSET and key not in _SEEDED:
-            # untimed, once per stream: a call of >= 65536 units seeds all 8192 MT19937
-            # generators; later samples continue the same streams
-            warm = [np.empty(1 << 18, dtype=dt) for _ in range(threads)]
-
-            def seed_all(i):
-                return fn(gens[i], c_void_p(warm[i].ctypes.data), c_size_t(1 << 18), *args)
-
             with ThreadPoolExecutor(threads) as ex:
-                assert all(s == 0 for s in ex.map(seed_all, range(threads)))
-            del warm
+                assert all(s == 0 for s in ex.map(lambda i: work(i, gens, view), range(threads)))
             _SEEDED[key] = gens
-
-        def work(i):
-            a, b = bounds[i]
-            return fn(gens[i], c_void_p(view[a:b].ctypes.data), c_size_t(b - a), *args)
-
+        gens = _SEEDED[key]
         t0 = time.perf_counter()
         with ThreadPoolExecutor(threads) as ex:
-            sts = list(ex.map(work, range(threads)))
+            sts = list(ex.map(lambda i: work(i, gens, view), range(threads)))
         t_all += time.perf_counter() - t0
         assert all(s == 0 for s in sts), sts
-        if gtype not in NO_OFFSET:
-            for g in gens:
-                lib.destroy(g)
         total_bytes += n_per_call * buf.itemsize
     return total_bytes, t_all, kind
 
@@ -1031,11 +1024,12 @@ def run_reference(args):
         return
     calls = select_calls(args.only)
     threads = os.cpu_count() or 1
-    # each step a bounded sample of the sweep (2^22 values per call, 1/64 of the GPU's 2^28),
-    # so that the default 20 + 5 steps end within a few minutes
-    step_n = max(1 << 16, args.cpu_n // 4)
+    # each step a bounded sample of the sweep (2^23 values per call, 1/32 of the GPU's 2^28),
+    # so that the default 20 + 5 steps end within a few minutes; the first sample of each
+    # call creates and warms its generators untimed
+    step_n = args.cpu_n
     for _ in range(args.warmup):
-        cpu_sample(step_n // 4, calls, threads)
+        cpu_sample(step_n, calls, threads)
     nb = 0
     secs = 0.0
     kind = None
@@ -1074,7 +1068,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 28)
-    ap.add_argument("--cpu-n", type=int, default=1 << 24)
+    ap.add_argument("--cpu-n", type=int, default=1 << 23)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="", help="gen:dist[:param],... subset of the sweep")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-fill and serving legs")

@@ -16,6 +16,7 @@
 
 #include <type_traits>
 #include "common.hpp"
+#include "ieee.cuh"
 #include "precise_math.cuh"
 
 #include <cuda_fp16.h>
@@ -39,105 +40,105 @@ namespace rb200
 // ---- scalar conversions ----
 
 // rocrand_uniform.h:61-64: 2^-32 + v * 2^-32 (exact product, one rounding).
-__device__ __forceinline__ float u32_to_f32(uint32_t v)
+RB_HD float u32_to_f32(uint32_t v)
 {
-    return __fmaf_rn(__uint2float_rn(v), RB_2POW32_INV, RB_2POW32_INV);
+    return ieee::ffma(ieee::u2f(v), RB_2POW32_INV, RB_2POW32_INV);
 }
 
 // rocrand_uniform.h:97-107: 53 bits from (v1, v2 >> 11), 2^-53 + v * 2^-53.
-__device__ __forceinline__ double u32x2_to_f64(uint32_t v1, uint32_t v2)
+RB_HD double u32x2_to_f64(uint32_t v1, uint32_t v2)
 {
     const uint64_t v = (uint64_t)v1 | ((uint64_t)(v2 >> 11) << 32);
-    return __fma_rn(__ull2double_rn(v), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+    return ieee::dfma(ieee::ull2d(v), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
 }
 
 // rocrand_uniform.h:92-95: 2^-32 + v * 2^-32 in double (exact).
-__device__ __forceinline__ double u32_to_f64(uint32_t v)
+RB_HD double u32_to_f64(uint32_t v)
 {
-    return __fma_rn(__uint2double_rn(v), RB_2POW32_INV_DOUBLE, RB_2POW32_INV_DOUBLE);
+    return ieee::dfma(ieee::u2d(v), RB_2POW32_INV_DOUBLE, RB_2POW32_INV_DOUBLE);
 }
 
 // rocrand_uniform.h:150-153: half of 2^-16 + v * 2^-16 (float math exact, RNE to half).
-__device__ __forceinline__ __half u16_to_f16(uint32_t v16)
+RB_HD __half u16_to_f16(uint32_t v16)
 {
-    return __float2half_rn(__fmaf_rn((float)(v16 & 0xffffu), RB_2POW16_INV, RB_2POW16_INV));
+    return __float2half_rn(ieee::ffma((float)(v16 & 0xffffu), RB_2POW16_INV, RB_2POW16_INV));
 }
 
 // rocrand_normal.h:51-66 (host branch: sinf/cosf on the rounded angle).
-__device__ __forceinline__ float2 box_muller_f32(uint32_t x, uint32_t y)
+RB_HD float2 box_muller_f32(uint32_t x, uint32_t y)
 {
-    const float u = __fmaf_rn(__uint2float_rn(x), RB_2POW32_INV, RB_2POW32_INV);
-    const float v = __fadd_rn(RB_2POW32_INV_2PI, __fmul_rn(__uint2float_rn(y), RB_2POW32_INV_2PI));
-    const float s = __fsqrt_rn(__fmul_rn(-2.0f, logf(u)));
+    const float u = ieee::ffma(ieee::u2f(x), RB_2POW32_INV, RB_2POW32_INV);
+    const float v = ieee::fadd(RB_2POW32_INV_2PI, ieee::fmul(ieee::u2f(y), RB_2POW32_INV_2PI));
+    const float s = ieee::fsqrt(ieee::fmul(-2.0f, ieee::logf_(u)));
     float       sv, cv;
-    sincosf(v, &sv, &cv);
-    return make_float2(__fmul_rn(sv, s), __fmul_rn(cv, s));
+    ieee::sincosf_(v, &sv, &cv);
+    return make_float2(ieee::fmul(sv, s), ieee::fmul(cv, s));
 }
 
 // rocrand_normal.h:68-89 (host branch: sin/cos of w * pi rounded in double).
-__device__ __forceinline__ double2 box_muller_f64(uint32_t x, uint32_t y, uint32_t z, uint32_t w)
+RB_HD double2 box_muller_f64(uint32_t x, uint32_t y, uint32_t z, uint32_t w)
 {
     const uint64_t v1 = (uint64_t)x ^ ((uint64_t)y << 21);
-    const double   u  = __fma_rn(__ull2double_rn(v1), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+    const double   u  = ieee::dfma(ieee::ull2d(v1), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
     const uint64_t v2 = (uint64_t)z ^ ((uint64_t)w << 21);
-    const double   ww = __fma_rn(__ull2double_rn(v2), RB_2POW53_INV_DOUBLE * 2.0, RB_2POW53_INV_DOUBLE * 2.0);
-    const double   s  = __dsqrt_rn(__dmul_rn(-2.0, pm::log(u)));
-    const double   a  = __dmul_rn(ww, RB_PI_DOUBLE);
+    const double   ww = ieee::dfma(ieee::ull2d(v2), RB_2POW53_INV_DOUBLE * 2.0, RB_2POW53_INV_DOUBLE * 2.0);
+    const double   s  = ieee::dsqrt(ieee::dmul(-2.0, pm::log(u)));
+    const double   a  = ieee::dmul(ww, RB_PI_DOUBLE);
     double         sv, cv;
     pm::sincos(a, sv, cv);
-    return make_double2(__dmul_rn(sv, s), __dmul_rn(cv, s));
+    return make_double2(ieee::dmul(sv, s), ieee::dmul(cv, s));
 }
 
 // rocrand_normal.h:102-122, float branch used by the host build; halves of the results.
-__device__ __forceinline__ void box_muller_f16(uint32_t v, __half r[2])
+RB_HD void box_muller_f16(uint32_t v, __half r[2])
 {
-    const float u = __fmaf_rn((float)(v & 0xffffu), RB_2POW16_INV, RB_2POW16_INV);
-    const float a = __fadd_rn(RB_2POW16_INV_2PI, __fmul_rn((float)(v >> 16), RB_2POW16_INV_2PI));
-    const float s = __fsqrt_rn(__fmul_rn(-2.0f, logf(u)));
+    const float u = ieee::ffma((float)(v & 0xffffu), RB_2POW16_INV, RB_2POW16_INV);
+    const float a = ieee::fadd(RB_2POW16_INV_2PI, ieee::fmul((float)(v >> 16), RB_2POW16_INV_2PI));
+    const float s = ieee::fsqrt(ieee::fmul(-2.0f, ieee::logf_(u)));
     float       sv, cv;
-    sincosf(a, &sv, &cv);
-    r[0] = __float2half_rn(__fmul_rn(sv, s));
-    r[1] = __float2half_rn(__fmul_rn(cv, s));
+    ieee::sincosf_(a, &sv, &cv);
+    r[0] = __float2half_rn(ieee::fmul(sv, s));
+    r[1] = __float2half_rn(ieee::fmul(cv, s));
 }
 
 // rocrand_normal.h:196-220 roc_d_erfinv (host branch).
-__device__ __forceinline__ double erfinv_d(double x)
+RB_HD double erfinv_d(double x)
 {
     const double sgn = (x < 0.0) ? -1.0 : 1.0;
-    x                = __dmul_rn(__dsub_rn(1.0, x), __dadd_rn(1.0, x));
+    x                = ieee::dmul(ieee::dsub(1.0, x), ieee::dadd(1.0, x));
     const double lnx = pm::log(x);
     if(isnan(lnx))
         return 1.0;
     if(isinf(lnx))
         return 0.0;
-    const double tt1 = __dadd_rn(2.0 / (RB_PI_DOUBLE * 0.147), __dmul_rn(0.5, lnx));
-    const double tt2 = __dmul_rn(1.0 / (0.147), lnx);
-    return sgn * __dsqrt_rn(__dadd_rn(-tt1, __dsqrt_rn(__dsub_rn(__dmul_rn(tt1, tt1), tt2))));
+    const double tt1 = ieee::dadd(2.0 / (RB_PI_DOUBLE * 0.147), ieee::dmul(0.5, lnx));
+    const double tt2 = ieee::dmul(1.0 / (0.147), lnx);
+    return sgn * ieee::dsqrt(ieee::dadd(-tt1, ieee::dsqrt(ieee::dsub(ieee::dmul(tt1, tt1), tt2))));
 }
 
 // rocrand_normal.h:265-270: sqrt(2) is a float literal promoted to double.
-__device__ __forceinline__ double normal_from_u32_f64(uint32_t x)
+RB_HD double normal_from_u32_f64(uint32_t x)
 {
     const double p = u32_to_f64(x);
-    return __dmul_rn((double)RB_SQRT2, erfinv_d(__dsub_rn(__dmul_rn(2.0, p), 1.0)));
+    return ieee::dmul((double)RB_SQRT2, erfinv_d(ieee::dsub(ieee::dmul(2.0, p), 1.0)));
 }
 
 // rocrand_discrete.h:33-60 discrete_alias for a 32-bit input.
-__device__ __forceinline__ uint32_t alias_lookup(uint32_t r, uint32_t size, uint32_t offset,
+RB_HD uint32_t alias_lookup(uint32_t r, uint32_t size, uint32_t offset,
                                                  const double* prob, const uint32_t* alias)
 {
-    const double   x   = __dmul_rn(__uint2double_rn(r), RB_2POW32_INV_DOUBLE);
-    const double   nx  = __dmul_rn(__uint2double_rn(size), x);
+    const double   x   = ieee::dmul(ieee::u2d(r), RB_2POW32_INV_DOUBLE);
+    const double   nx  = ieee::dmul(ieee::u2d(size), x);
     const double   fnx = floor(nx);
-    const double   y   = __dsub_rn(nx, fnx);
-    const uint32_t i   = __double2uint_rz(fnx);
+    const double   y   = ieee::dsub(nx, fnx);
+    const uint32_t i   = ieee::d2u_rz(fnx);
     return offset + (y < prob[i] ? i : alias[i]);
 }
 
 // The same pick from packed integer entries (poisson.hpp alias_entry: threshold in the low
 // 33 bits, alias above): i = (size r) >> 32, entry i when the low word of size r is below
 // the threshold.  One 8-byte read, no conversion or fp64 operation.
-__device__ __forceinline__ uint32_t alias_lookup_packed(uint32_t r, uint32_t size, uint32_t offset,
+RB_HD uint32_t alias_lookup_packed(uint32_t r, uint32_t size, uint32_t offset,
                                                         const unsigned long long* tab)
 {
     const unsigned long long p  = static_cast<unsigned long long>(size) * r;
@@ -148,10 +149,10 @@ __device__ __forceinline__ uint32_t alias_lookup_packed(uint32_t r, uint32_t siz
 }
 
 // poisson.hpp:80-108 poisson_distribution_huge: round(sqrt(lambda) * N + lambda).
-__device__ __forceinline__ uint32_t poisson_huge(uint32_t r, double sqrt_lambda, double lambda)
+RB_HD uint32_t poisson_huge(uint32_t r, double sqrt_lambda, double lambda)
 {
     const double nd = normal_from_u32_f64(r);
-    return (uint32_t)(long long)round(__dadd_rn(__dmul_rn(sqrt_lambda, nd), lambda));
+    return (uint32_t)(long long)round(ieee::dadd(ieee::dmul(sqrt_lambda, nd), lambda));
 }
 
 // ---- functors: iw inputs (32-bit engine words) -> ow outputs of T ----
@@ -161,14 +162,14 @@ struct FnUint // uniform_distribution<uint> (uniform.hpp:42-53)
 {
     using T                      = uint32_t;
     static constexpr unsigned iw = 1, ow = 1;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const { out[0] = in[0]; }
+    RB_HD void operator()(const uint32_t* in, T* out) const { out[0] = in[0]; }
 };
 
 struct FnUchar // uniform_distribution<uchar> (uniform.hpp:55-66): the word's 4 bytes
 {
     using T                      = uint8_t;
     static constexpr unsigned iw = 1, ow = 4;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = (uint8_t)in[0];
         out[1] = (uint8_t)(in[0] >> 8);
@@ -181,7 +182,7 @@ struct FnUshort // uniform_distribution<ushort> (uniform.hpp:68-79): the word's 
 {
     using T                      = uint16_t;
     static constexpr unsigned iw = 1, ow = 2;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = (uint16_t)in[0];
         out[1] = (uint16_t)(in[0] >> 16);
@@ -192,7 +193,7 @@ struct FnFloat // uniform_distribution<float> (uniform.hpp:81-91)
 {
     using T                      = float;
     static constexpr unsigned iw = 1, ow = 1;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = u32_to_f32(in[0]);
     }
@@ -202,7 +203,7 @@ struct FnDouble // uniform_distribution<double> (uniform.hpp:93-103)
 {
     using T                      = double;
     static constexpr unsigned iw = 2, ow = 1;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = u32x2_to_f64(in[0], in[1]);
     }
@@ -212,7 +213,7 @@ struct FnHalf // uniform_distribution<half> (uniform.hpp:105-117)
 {
     using T                      = __half;
     static constexpr unsigned iw = 1, ow = 2;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = u16_to_f16(in[0] & 0xffffu);
         out[1] = u16_to_f16(in[0] >> 16);
@@ -224,11 +225,11 @@ struct FnNormalF // normal_distribution<float, uint, 4> (normal.hpp:49-69)
     using T                      = float;
     static constexpr unsigned iw = 2, ow = 2;
     float                     mean, stddev;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         const float2 v = box_muller_f32(in[0], in[1]);
-        out[0]         = __fadd_rn(mean, __fmul_rn(v.x, stddev));
-        out[1]         = __fadd_rn(mean, __fmul_rn(v.y, stddev));
+        out[0]         = ieee::fadd(mean, ieee::fmul(v.x, stddev));
+        out[1]         = ieee::fadd(mean, ieee::fmul(v.y, stddev));
     }
 };
 
@@ -237,11 +238,11 @@ struct FnLogNormalF // log_normal_distribution<float, uint, 4> (log_normal.hpp:5
     using T                      = float;
     static constexpr unsigned iw = 2, ow = 2;
     float                     mean, stddev;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         const float2 v = box_muller_f32(in[0], in[1]);
-        out[0]         = expf(__fadd_rn(mean, __fmul_rn(v.x, stddev)));
-        out[1]         = expf(__fadd_rn(mean, __fmul_rn(v.y, stddev)));
+        out[0]         = ieee::expf_(ieee::fadd(mean, ieee::fmul(v.x, stddev)));
+        out[1]         = ieee::expf_(ieee::fadd(mean, ieee::fmul(v.y, stddev)));
     }
 };
 
@@ -250,11 +251,11 @@ struct FnNormalD // normal_distribution<double, uint, 4> (normal.hpp:90-111)
     using T                      = double;
     static constexpr unsigned iw = 4, ow = 2;
     double                    mean, stddev;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         const double2 v = box_muller_f64(in[0], in[1], in[2], in[3]);
-        out[0]          = __dadd_rn(mean, __dmul_rn(v.x, stddev));
-        out[1]          = __dadd_rn(mean, __dmul_rn(v.y, stddev));
+        out[0]          = ieee::dadd(mean, ieee::dmul(v.x, stddev));
+        out[1]          = ieee::dadd(mean, ieee::dmul(v.y, stddev));
     }
 };
 
@@ -263,11 +264,11 @@ struct FnLogNormalD // log_normal_distribution<double, uint, 4> (log_normal.hpp:
     using T                      = double;
     static constexpr unsigned iw = 4, ow = 2;
     double                    mean, stddev;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         const double2 v = box_muller_f64(in[0], in[1], in[2], in[3]);
-        out[0]          = exp(__dadd_rn(mean, __dmul_rn(v.x, stddev)));
-        out[1]          = exp(__dadd_rn(mean, __dmul_rn(v.y, stddev)));
+        out[0]          = ieee::exp_(ieee::dadd(mean, ieee::dmul(v.x, stddev)));
+        out[1]          = ieee::exp_(ieee::dadd(mean, ieee::dmul(v.y, stddev)));
     }
 };
 
@@ -276,12 +277,12 @@ struct FnNormalH // normal_distribution<half, uint, 4> (normal.hpp:113-136), flo
     using T                      = __half;
     static constexpr unsigned iw = 1, ow = 2;
     float                     mean, stddev; // the half parameters widened to float
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         __half r[2];
         box_muller_f16(in[0], r);
-        out[0] = __float2half_rn(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[0]))));
-        out[1] = __float2half_rn(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[1]))));
+        out[0] = __float2half_rn(ieee::fadd(mean, ieee::fmul(stddev, __half2float(r[0]))));
+        out[1] = __float2half_rn(ieee::fadd(mean, ieee::fmul(stddev, __half2float(r[1]))));
     }
 };
 
@@ -290,12 +291,12 @@ struct FnLogNormalH // log_normal_distribution<half, uint, 4> (log_normal.hpp:11
     using T                      = __half;
     static constexpr unsigned iw = 1, ow = 2;
     float                     mean, stddev;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         __half r[2];
         box_muller_f16(in[0], r);
-        out[0] = __float2half_rn(expf(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[0])))));
-        out[1] = __float2half_rn(expf(__fadd_rn(mean, __fmul_rn(stddev, __half2float(r[1])))));
+        out[0] = __float2half_rn(ieee::expf_(ieee::fadd(mean, ieee::fmul(stddev, __half2float(r[0])))));
+        out[1] = __float2half_rn(ieee::expf_(ieee::fadd(mean, ieee::fmul(stddev, __half2float(r[1])))));
     }
 };
 
@@ -309,7 +310,7 @@ struct FnPoisson
     const unsigned long long* prob;  // packed entries (alias_entry), not probabilities
     const uint32_t*           alias; // unused: the aliases are packed with the thresholds
     uint32_t                  size, offset;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = alias_lookup_packed(in[0], size, offset, prob);
     }
@@ -321,7 +322,7 @@ struct FnPoissonHuge
     using T                      = uint32_t;
     static constexpr unsigned iw = 1, ow = 1;
     double                    sqrt_lambda, lambda;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = poisson_huge(in[0], sqrt_lambda, lambda);
     }
@@ -335,7 +336,7 @@ struct Fn64Ulonglong // uniform_distribution<ull, ull>
 {
     using T                      = unsigned long long;
     static constexpr unsigned iw = 1, ow = 1;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
         out[0] = in[0];
     }
@@ -346,7 +347,7 @@ struct Fn64Split // uchar (ow 8), ushort (ow 4), uint (ow 2): the word's bytes i
 {
     using T                      = U;
     static constexpr unsigned iw = 1, ow = N;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
 #pragma unroll
         for(unsigned k = 0; k < N; k++)
@@ -358,7 +359,7 @@ struct Fn64Float // rocrand_uniform.h:66-69: 2^-32 + (v >> 32) * 2^-32
 {
     using T                      = float;
     static constexpr unsigned iw = 1, ow = 1;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
         out[0] = u32_to_f32(static_cast<uint32_t>(in[0] >> 32));
     }
@@ -368,9 +369,9 @@ struct Fn64Double // rocrand_uniform.h:109-116: 2^-53 + (v >> 11) * 2^-53
 {
     using T                      = double;
     static constexpr unsigned iw = 1, ow = 1;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
-        out[0] = __fma_rn(__ull2double_rn(in[0] >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+        out[0] = ieee::dfma(ieee::ull2d(in[0] >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
     }
 };
 
@@ -378,7 +379,7 @@ struct Fn64Half // uniform_distribution<half, ull>: four 16-bit fields
 {
     using T                      = __half;
     static constexpr unsigned iw = 1, ow = 4;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
 #pragma unroll
         for(unsigned k = 0; k < 4; k++)
@@ -392,13 +393,13 @@ struct Fn64NormalF // box_muller(unsigned long long): x = low word, y = high wor
     static constexpr unsigned iw = 1, ow = 2;
     float                     mean, stddev;
     bool                      log_normal;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
         const float2 v = box_muller_f32(static_cast<uint32_t>(in[0]), static_cast<uint32_t>(in[0] >> 32));
-        const float  a = __fadd_rn(mean, __fmul_rn(v.x, stddev));
-        const float  b = __fadd_rn(mean, __fmul_rn(v.y, stddev));
-        out[0]         = log_normal ? expf(a) : a;
-        out[1]         = log_normal ? expf(b) : b;
+        const float  a = ieee::fadd(mean, ieee::fmul(v.x, stddev));
+        const float  b = ieee::fadd(mean, ieee::fmul(v.y, stddev));
+        out[0]         = log_normal ? ieee::expf_(a) : a;
+        out[1]         = log_normal ? ieee::expf_(b) : b;
     }
 };
 
@@ -408,14 +409,14 @@ struct Fn64NormalD // box_muller_double(ulonglong2)
     static constexpr unsigned iw = 2, ow = 2;
     double                    mean, stddev;
     bool                      log_normal;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
         const double2 v = box_muller_f64(static_cast<uint32_t>(in[0]), static_cast<uint32_t>(in[0] >> 32),
                                          static_cast<uint32_t>(in[1]), static_cast<uint32_t>(in[1] >> 32));
-        const double  a = __dadd_rn(mean, __dmul_rn(v.x, stddev));
-        const double  b = __dadd_rn(mean, __dmul_rn(v.y, stddev));
-        out[0]          = log_normal ? exp(a) : a;
-        out[1]          = log_normal ? exp(b) : b;
+        const double  a = ieee::dadd(mean, ieee::dmul(v.x, stddev));
+        const double  b = ieee::dadd(mean, ieee::dmul(v.y, stddev));
+        out[0]          = log_normal ? ieee::exp_(a) : a;
+        out[1]          = log_normal ? ieee::exp_(b) : b;
     }
 };
 
@@ -425,7 +426,7 @@ struct Fn64NormalH // normal_distribution_half2(ull): (ushort)v and (ushort)(v >
     static constexpr unsigned iw = 1, ow = 2;
     float                     mean, stddev;
     bool                      log_normal;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
         __half         r[2];
         const uint32_t v = (static_cast<uint32_t>(in[0]) & 0xffffu)
@@ -434,8 +435,8 @@ struct Fn64NormalH // normal_distribution_half2(ull): (ushort)v and (ushort)(v >
 #pragma unroll
         for(int k = 0; k < 2; k++)
         {
-            const float z = __fadd_rn(mean, __fmul_rn(stddev, __half2float(r[k])));
-            out[k]        = __float2half_rn(log_normal ? expf(z) : z);
+            const float z = ieee::fadd(mean, ieee::fmul(stddev, __half2float(r[k])));
+            out[k]        = __float2half_rn(log_normal ? ieee::expf_(z) : z);
         }
     }
 };
@@ -450,13 +451,13 @@ struct Fn64Poisson
     const double*             prob;
     const uint32_t*           alias;
     uint32_t                  size, offset;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
-        const double x   = __dmul_rn(__ull2double_rn(in[0]), 5.4210108624275221700372640043497e-20);
-        const double nx  = __dmul_rn(__uint2double_rn(size), x);
+        const double x   = ieee::dmul(ieee::ull2d(in[0]), 5.4210108624275221700372640043497e-20);
+        const double nx  = ieee::dmul(ieee::u2d(size), x);
         const double fnx = floor(nx);
-        const double y   = __dsub_rn(nx, fnx);
-        uint32_t     i   = __double2uint_rz(fnx);
+        const double y   = ieee::dsub(nx, fnx);
+        uint32_t     i   = ieee::d2u_rz(fnx);
         i                = i < size ? i : size - 1;
         out[0]           = offset + (y < prob[i] ? i : alias[i]);
     }
@@ -467,11 +468,11 @@ struct Fn64PoissonHuge // normal_distribution_double(ull) then round(sqrt(l) * N
     using T                      = uint32_t;
     static constexpr unsigned iw = 1, ow = 1;
     double                    sqrt_lambda, lambda;
-    __device__ __forceinline__ void operator()(const unsigned long long* in, T* out) const
+    RB_HD void operator()(const unsigned long long* in, T* out) const
     {
-        const double p  = __fma_rn(__ull2double_rn(in[0] >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
-        const double nd = __dmul_rn((double)RB_SQRT2, erfinv_d(__dsub_rn(__dmul_rn(2.0, p), 1.0)));
-        out[0]          = (uint32_t)(long long)round(__dadd_rn(__dmul_rn(sqrt_lambda, nd), lambda));
+        const double p  = ieee::dfma(ieee::ull2d(in[0] >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+        const double nd = ieee::dmul((double)RB_SQRT2, erfinv_d(ieee::dsub(ieee::dmul(2.0, p), 1.0)));
+        out[0]          = (uint32_t)(long long)round(ieee::dadd(ieee::dmul(sqrt_lambda, nd), lambda));
     }
 };
 
@@ -483,10 +484,10 @@ struct FnNormalD1
     static constexpr unsigned iw = 1, ow = 1;
     double                    mean, stddev;
     bool                      log_normal;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
-        const double z = __dadd_rn(mean, __dmul_rn(normal_from_u32_f64(in[0]), stddev));
-        out[0]         = log_normal ? exp(z) : z;
+        const double z = ieee::dadd(mean, ieee::dmul(normal_from_u32_f64(in[0]), stddev));
+        out[0]         = log_normal ? ieee::exp_(z) : z;
     }
 };
 
@@ -506,19 +507,19 @@ struct Mrg32k3aNorm // rocrand_mrg32k3a.h:38-39
 };
 
 template<class N>
-__device__ __forceinline__ uint32_t mrg_to_u32(uint32_t v) // (v - 1) * UINT_NORM, truncated
+RB_HD uint32_t mrg_to_u32(uint32_t v) // (v - 1) * UINT_NORM, truncated
 {
-    return __double2uint_rz(__dmul_rn(__uint2double_rn(v - 1u), N::kUintNorm));
+    return ieee::d2u_rz(ieee::dmul(ieee::u2d(v - 1u), N::kUintNorm));
 }
 template<class N>
-__device__ __forceinline__ float mrg_to_f32(uint32_t v)
+RB_HD float mrg_to_f32(uint32_t v)
 {
-    return __double2float_rn(__dmul_rn(__uint2double_rn(v), N::kNorm));
+    return ieee::d2f(ieee::dmul(ieee::u2d(v), N::kNorm));
 }
 template<class N>
-__device__ __forceinline__ double mrg_to_f64(uint32_t v)
+RB_HD double mrg_to_f64(uint32_t v)
 {
-    return __dmul_rn(__uint2double_rn(v), N::kNorm);
+    return ieee::dmul(ieee::u2d(v), N::kNorm);
 }
 
 template<class N, class Inner>
@@ -527,7 +528,7 @@ struct FnMrgRemap // uint/uchar/ushort/half/Poisson: remap to [0, 2^32) then the
     using T                      = typename Inner::T;
     static constexpr unsigned iw = 1, ow = Inner::ow;
     Inner                     inner;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         const uint32_t v = mrg_to_u32<N>(in[0]);
         inner(&v, out);
@@ -539,7 +540,7 @@ struct FnMrgFloat
 {
     using T                      = float;
     static constexpr unsigned iw = 1, ow = 1;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = mrg_to_f32<N>(in[0]);
     }
@@ -550,7 +551,7 @@ struct FnMrgDouble
 {
     using T                      = double;
     static constexpr unsigned iw = 1, ow = 1;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = mrg_to_f64<N>(in[0]);
     }
@@ -563,17 +564,17 @@ struct FnMrgNormalF // mrg_box_muller (rocrand_normal.h:138-152)
     static constexpr unsigned iw = 2, ow = 2;
     float                     mean, stddev;
     bool                      log_normal;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         const float u = mrg_to_f32<N>(in[0]);
-        const float v = __fmul_rn(mrg_to_f32<N>(in[1]), 6.2831855f);
-        const float s = __fsqrt_rn(__fmul_rn(-2.0f, logf(u)));
+        const float v = ieee::fmul(mrg_to_f32<N>(in[1]), 6.2831855f);
+        const float s = ieee::fsqrt(ieee::fmul(-2.0f, ieee::logf_(u)));
         float       sv, cv;
-        sincosf(v, &sv, &cv);
-        const float a = __fadd_rn(mean, __fmul_rn(__fmul_rn(sv, s), stddev));
-        const float b = __fadd_rn(mean, __fmul_rn(__fmul_rn(cv, s), stddev));
-        out[0]        = log_normal ? expf(a) : a;
-        out[1]        = log_normal ? expf(b) : b;
+        ieee::sincosf_(v, &sv, &cv);
+        const float a = ieee::fadd(mean, ieee::fmul(ieee::fmul(sv, s), stddev));
+        const float b = ieee::fadd(mean, ieee::fmul(ieee::fmul(cv, s), stddev));
+        out[0]        = log_normal ? ieee::expf_(a) : a;
+        out[1]        = log_normal ? ieee::expf_(b) : b;
     }
 };
 
@@ -584,17 +585,17 @@ struct FnMrgNormalD // mrg_box_muller_double (rocrand_normal.h:154-172): float u
     static constexpr unsigned iw = 2, ow = 2;
     double                    mean, stddev;
     bool                      log_normal;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         const double u = (double)mrg_to_f32<N>(in[0]);
         const double v = (double)mrg_to_f32<N>(in[1]) * 2.0;
-        const double s = __dsqrt_rn(__dmul_rn(-2.0, pm::log(u)));
+        const double s = ieee::dsqrt(ieee::dmul(-2.0, pm::log(u)));
         double       sv, cv;
-        pm::sincos(__dmul_rn(v, RB_PI_DOUBLE), sv, cv);
-        const double a = __dadd_rn(mean, __dmul_rn(__dmul_rn(sv, s), stddev));
-        const double b = __dadd_rn(mean, __dmul_rn(__dmul_rn(cv, s), stddev));
-        out[0]         = log_normal ? exp(a) : a;
-        out[1]         = log_normal ? exp(b) : b;
+        pm::sincos(ieee::dmul(v, RB_PI_DOUBLE), sv, cv);
+        const double a = ieee::dadd(mean, ieee::dmul(ieee::dmul(sv, s), stddev));
+        const double b = ieee::dadd(mean, ieee::dmul(ieee::dmul(cv, s), stddev));
+        out[0]         = log_normal ? ieee::exp_(a) : a;
+        out[1]         = log_normal ? ieee::exp_(b) : b;
     }
 };
 
@@ -604,7 +605,7 @@ struct FnMrgPoissonHuge
     using T                      = uint32_t;
     static constexpr unsigned iw = 1, ow = 1;
     double                    sqrt_lambda, lambda;
-    __device__ __forceinline__ void operator()(const uint32_t* in, T* out) const
+    RB_HD void operator()(const uint32_t* in, T* out) const
     {
         out[0] = poisson_huge(mrg_to_u32<N>(in[0]), sqrt_lambda, lambda);
     }

@@ -15,14 +15,14 @@
 // build (rocrand_b200/data/make_logf_replay.cpp) runs the host's logf over every argument
 // the formula can reach and records
 //  * per bucket of arguments (the float's bits >> kBucketShift), the largest distance from
-//    the midpoint, in units of 2^-16 ulp, of an argument where the host's result differs
-//    from f (0: none in the bucket);
+//    the midpoint, in units of 2^-16 ulp (plus one), of an argument where the host's result
+//    differs from f (0: none in the bucket);
 //  * the differing arguments with the host's result, in an open-addressing hash table.
 // An argument whose distance is within its bucket's bound looks itself up (a few percent of
 // arguments); all others return f.  The build then replays every reachable argument through
-// this same code on the host and requires the host's logf result for each.  f, the
-// distance and the lookup are IEEE operations only, so the host and device builds of this
-// header agree bit for bit.
+// this same code on the host and requires the host's logf result for each.  f is IEEE
+// operations only and the distance and lookup integer ones, so the host and device builds
+// of this header agree bit for bit.
 #pragma once
 
 #include "precise_math.cuh"
@@ -62,33 +62,19 @@ RB_PM_HD float ffrom(uint32_t u)
     return x;
 }
 
-// The float next to f in direction `up` (f finite).
-RB_PM_HD float step(float f, bool up)
+// The device's own float logarithm f of t, and the distance of its double value L from the
+// rounding boundary between the two floats around L, in units of 2^-16 float ulp (0 ..
+// 32768; larger = safer).  L's double mantissa carries 29 bits below the float's last bit;
+// they place L between the two floats (|L| > 2^-26 here, so L is a normal float number and
+// both floats share its exponent or the larger one is the next power of two), and the
+// boundary sits at 2^28 of them: integer operations only.
+RB_PM_HD float base(float t, uint32_t& dist)
 {
-    if(f == 0.0f)
-        return up ? ffrom(1u) : ffrom(0x80000001u);
-    const uint32_t u = fbits(f);
-    return ffrom((f > 0.0f) == up ? u + 1u : u - 1u);
-}
-
-// The device's own float logarithm f of t, and the distance of the accurate value from the
-// rounding boundary between f and its neighbour on that side, in units of 2^-16 ulp
-// (0 .. 32768; larger = safer).  t must be finite and positive.
-RB_PM_HD float base(float t, double& dist)
-{
-    const double L  = pm::log_unit(static_cast<double>(t));
-    const float  f  = static_cast<float>(L);
-    const double fd = static_cast<double>(f);
-    const float  nb = step(f, L > fd);
-    const double nd = static_cast<double>(nb);
-    const double mid = 0.5 * (fd + nd);                 // exact
-    const double ulp = nd > fd ? nd - fd : fd - nd;     // exact, a power of two
-    const double gap = L > mid ? L - mid : mid - L;
-    // 2^16 / ulp built from ulp's exponent (an exact power of two, no division)
-    const uint64_t e     = (pm::bits_of(ulp) >> 52) & 0x7ff;
-    const double   scale = pm::from_bits((2046ull + 16ull - e) << 52);
-    dist                 = gap * scale;
-    return f;
+    const double   L   = pm::log_unit(static_cast<double>(t));
+    const uint32_t low = static_cast<uint32_t>(pm::bits_of(L)) & 0x1fffffffu;
+    const uint32_t off = low > (1u << 28) ? low - (1u << 28) : (1u << 28) - low;
+    dist               = off >> 13;
+    return static_cast<float>(L);
 }
 
 // The host C library's logf(t) for an argument of the inverse-erf normal.
@@ -96,7 +82,7 @@ RB_PM_HD float logf_host(float t, const Table& tb)
 {
     if(!(t > 0.0f) || !(t <= 1.0f))
         return pm::logf(t); // zero (-inf) and anything outside the formula's range
-    double      dist;
+    uint32_t    dist;
     const float f   = base(t, dist);
     const uint32_t key = fbits(t);
 #if defined(__CUDA_ARCH__)
@@ -104,7 +90,7 @@ RB_PM_HD float logf_host(float t, const Table& tb)
 #else
     const uint32_t bound = tb.bound[key >> kBucketShift];
 #endif
-    if(bound == 0u || dist > static_cast<double>(bound))
+    if(bound == 0u || dist > bound)
         return f;
     const uint32_t mask = (1u << tb.log2_slots) - 1u;
     uint32_t       h    = (key * kHashMul) >> (32 - tb.log2_slots);

@@ -68,7 +68,7 @@ int main(int argc, char** argv)
     const size_t          na = args.size();
     std::vector<uint32_t> host(na);
     std::vector<uint8_t>  differs(na, 0);
-    std::vector<double>   dist(na, 0.0);
+    std::vector<uint32_t> dist(na, 0);
 #pragma omp parallel for schedule(dynamic, 4096)
     for(long long i = 0; i < static_cast<long long>(na); i++)
     {
@@ -79,7 +79,7 @@ int main(int argc, char** argv)
             differs[i] = lr::fbits(pm::logf(t)) != host[i] ? 2 : 0; // must not happen
             continue;
         }
-        double      d;
+        uint32_t    d;
         const float f = lr::base(t, d);
         dist[i]       = d;
         differs[i]    = lr::fbits(f) != host[i] ? 1 : 0;
@@ -96,7 +96,7 @@ int main(int argc, char** argv)
         if(differs[i] == 0)
             continue;
         const uint32_t key = args[i] >> lr::kBucketShift;
-        const double   b   = std::ceil(dist[i]) + 1.0;
+        const double   b   = static_cast<double>(dist[i]) + 1.0;
         if(key >= lr::kBuckets || b > 65535.0)
         {
             std::fprintf(stderr, "argument %08x: bucket %u, bound %.1f out of range\n", args[i], key, b);
