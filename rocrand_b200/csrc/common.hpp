@@ -140,6 +140,13 @@ struct rocrand_generator_base_type
 
     cudaStream_t stream() const { return m_stream; }
 
+    // Host execution: generate calls write host memory, computed on the CPU by the same
+    // engine and distribution code as the kernels (host generators of a process with no GPU,
+    // host_generator.cpp).  Families without a CPU form return false.
+    virtual bool set_host_execution() { return false; }
+    bool         host_execution() const { return m_host_exec; }
+
 protected:
-    cudaStream_t m_stream = 0;
+    cudaStream_t m_stream    = 0;
+    bool         m_host_exec = false;
 };

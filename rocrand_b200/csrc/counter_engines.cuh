@@ -42,7 +42,7 @@ inline PhiloxKeys philox_keys(unsigned long long seed)
 }
 
 // Ten Philox rounds of one 128-bit counter (Random123's S-box: two 32x32->64 products).
-__device__ __forceinline__ uint4 philox_block(uint4 c, const PhiloxKeys& pk)
+__host__ __device__ __forceinline__ uint4 philox_block(uint4 c, const PhiloxKeys& pk)
 {
 #pragma unroll
     for(int r = 0; r < 10; r++)
@@ -132,7 +132,7 @@ struct CounterPos
 };
 
 // Words s..s+3 of the 8-word concatenation (a, b): the engine's interleave.
-__device__ __forceinline__ uint4 interleave4(uint4 a, uint4 b, uint32_t s)
+__host__ __device__ __forceinline__ uint4 interleave4(uint4 a, uint4 b, uint32_t s)
 {
     switch(s)
     {
@@ -143,7 +143,7 @@ __device__ __forceinline__ uint4 interleave4(uint4 a, uint4 b, uint32_t s)
     }
 }
 
-__device__ __forceinline__ uint32_t word_of(uint4 v, uint32_t i)
+__host__ __device__ __forceinline__ uint32_t word_of(uint4 v, uint32_t i)
 {
     switch(i)
     {

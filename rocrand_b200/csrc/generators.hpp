@@ -27,6 +27,14 @@ public:
     }
 
 protected:
+    // Host execution for a family that has a CPU form: tables stay on the host.
+    bool enable_host()
+    {
+        m_host_exec = true;
+        m_poisson.set_host();
+        return true;
+    }
+
     unsigned long long m_seed        = 0;
     unsigned long long m_offset      = 0;
     rocrand_ordering   m_order       = ROCRAND_ORDERING_PSEUDO_DEFAULT;
@@ -47,6 +55,7 @@ public:
     rocrand_status   generate_poisson(unsigned int* data, size_t n, double lambda) override;
     rocrand_status   batch_descriptor(uint32_t dist, double p0, double p1, void* data, size_t n,
                                       BatchReq& r, cudaStream_t stream) override;
+    bool             set_host_execution() override { return enable_host(); }
 
 private:
     CounterPos m_pos;

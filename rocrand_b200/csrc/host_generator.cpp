@@ -1,19 +1,26 @@
 // host_generator.cpp -- rocrand_create_generator_host / _host_blocking.
 //
 // The reference's host generators write into host memory with the same values as its
-// device generators (library/src/rng/generator_type.hpp:128-177, rocrand.cpp:111-160).
-// Here a host generator is a device generator of the same type whose outputs are copied
-// into the caller's host buffer: each generate call runs the device kernel into a scratch
-// buffer that has the same address modulo 256 bytes as the host buffer (the output layout
-// -- head, aligned vectors, tail -- depends on the address), then copies the n values out
-// on the generator's stream and waits for them.  So the non-blocking flavour returns with
-// its outputs complete as the blocking one does, which its contract allows.
+// device generators (library/src/rng/generator_type.hpp:128-177, rocrand.cpp:111-160), and
+// run on the CPU (system.hpp:140-214).  Here a host generator takes one of two forms:
+//  * in a process with no CUDA device (or with ROCRAND_B200_HOST_CPU=1 in the environment),
+//    the generator itself in host execution: every generate call runs on the CPU, through
+//    the same engine, output-order and distribution code as the kernels (compiled for the
+//    host; fp32 transcendentals from the C library, as the reference's host path takes
+//    them), spread over the host's cores;
+//  * otherwise the device generator of the same type, whose outputs are copied into the
+//    caller's host buffer: each generate call runs the device kernel into a scratch buffer
+//    that has the same address modulo 256 bytes as the host buffer (the output layout --
+//    head, aligned vectors, tail -- depends on the address), then copies the n values out
+//    on the generator's stream and waits for them.  So the non-blocking flavour returns
+//    with its outputs complete as the blocking one does, which its contract allows.
 #include "common.hpp"
 #include "generators.hpp"
 
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <memory>
 
 namespace rb200
@@ -107,11 +114,28 @@ private:
 
 } // namespace
 
+// No usable CUDA device, or host execution asked for.
+static bool host_cpu_mode()
+{
+    const char* e = std::getenv("ROCRAND_B200_HOST_CPU");
+    if(e != nullptr && e[0] != '\0' && e[0] != '0')
+        return true;
+    int count = 0;
+    if(cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    {
+        cudaGetLastError();
+        return true;
+    }
+    return false;
+}
+
 rocrand_generator_base_type* make_host_generator(rocrand_rng_type t)
 {
     rocrand_generator_base_type* inner = make_generator(t);
     if(inner == nullptr)
         return nullptr;
+    if(host_cpu_mode() && inner->set_host_execution())
+        return inner;
     return new HostGenerator(inner);
 }
 

@@ -22,7 +22,7 @@ __device__ __forceinline__ void store16_cs(void* p, uint4 v)
 
 // Packs ow*opt values of T (16 bytes) into a uint4.
 template<class T, unsigned N>
-__device__ __forceinline__ uint4 pack16(const T (&v)[N])
+__host__ __device__ __forceinline__ uint4 pack16(const T (&v)[N])
 {
     static_assert(sizeof(T) * N == 16, "16-byte vectors only");
     uint4 r;

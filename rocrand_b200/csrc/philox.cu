@@ -20,8 +20,11 @@
 #include "generators.hpp"
 #include "launch.cuh"
 #include "batch.hpp"
+#include "host_exec.hpp"
 #include "philox.cuh"
 #include "poisson.hpp"
+
+#include <cstring>
 
 namespace rb200
 {
@@ -110,6 +113,36 @@ __global__ void __launch_bounds__(kBlock)
             philox_scalar_run(a, g, 4 * a.vec_n + a.head, reinterpret_cast<T*>(a.data) + (a.n - a.tail),
                               a.tail);
     }
+}
+
+// The same output contract on the host (host generators without a GPU): every vector by
+// the general rule of philox_fill, the head and tail by the same sequential run.
+template<class F>
+static rocrand_status philox_run_host(const PhiloxCall& a, const F& f)
+{
+    host_parallel_for(a.vec_n, [&](unsigned long long j0, unsigned long long j1) {
+        for(unsigned long long j = j0; j < j1; j++)
+        {
+            const uint32_t           adj = (j & (kPhiloxRefStride - 1)) == 0 ? a.start0 : a.head;
+            const unsigned long long q   = a.s0 + adj + 4 * j;
+            const uint4              c   = ctr_add(a.c0, q >> 2);
+            const uint32_t           s   = static_cast<uint32_t>(q & 3);
+            uint4                    b   = philox_block(c, a.keys);
+            if(s != 0)
+                b = interleave4(b, philox_block(ctr_add(c, 1), a.keys), s);
+            const uint4 v = philox_vec(f, b);
+            std::memcpy(a.vec + j * 16, &v, 16);
+        }
+    });
+    using T = typename F::T;
+    if(a.head > 0)
+        philox_scalar_run(a, f, 0, reinterpret_cast<T*>(a.data), a.head);
+    if(a.tail > 0)
+    {
+        const unsigned long long pos = 4 * a.vec_n + ((a.vec_n % kPhiloxRefStride) == 0 ? a.start0 : a.head);
+        philox_scalar_run(a, f, pos, reinterpret_cast<T*>(a.data) + (a.n - a.tail), a.tail);
+    }
+    return ROCRAND_STATUS_SUCCESS;
 }
 
 template<class F>
@@ -227,7 +260,7 @@ rocrand_status PhiloxGenerator::generate(void* data, size_t n, Dist d, const Dis
         a.vec    = a.data + mis * tsize;
         if(n == 0)
             return ROCRAND_STATUS_SUCCESS;
-        const rocrand_status s = launch_philox(a, f, m_stream);
+        const rocrand_status s = m_host_exec ? philox_run_host(a, f) : launch_philox(a, f, m_stream);
         if(s == ROCRAND_STATUS_SUCCESS)
             m_pos.advance(static_cast<unsigned long long>((n + ow - 1) / ow) * iw);
         return s;

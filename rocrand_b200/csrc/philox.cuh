@@ -27,7 +27,7 @@ struct PhiloxCall
 };
 
 // Value at relative stream position p (sequential head/tail path only).
-__device__ __forceinline__ uint32_t philox_value(const PhiloxCall& a, unsigned long long p)
+__host__ __device__ __forceinline__ uint32_t philox_value(const PhiloxCall& a, unsigned long long p)
 {
     const unsigned long long q = a.s0 + p;
     const uint4              b = philox_block(ctr_add(a.c0, q >> 2), a.keys);
@@ -37,7 +37,7 @@ __device__ __forceinline__ uint32_t philox_value(const PhiloxCall& a, unsigned l
 // Applies F sequentially from stream position `pos` and writes `count` elements at `out`
 // (the reference's scalar head/tail loops, one engine() per input).
 template<class F>
-__device__ void philox_scalar_run(const PhiloxCall& a, const F& f, unsigned long long pos,
+__host__ __device__ void philox_scalar_run(const PhiloxCall& a, const F& f, unsigned long long pos,
                                   typename F::T* out, uint32_t count)
 {
     typename F::T v[F::ow];
@@ -53,7 +53,7 @@ __device__ void philox_scalar_run(const PhiloxCall& a, const F& f, unsigned long
 }
 
 template<class F>
-__device__ __forceinline__ uint4 philox_vec(const F& f, uint4 w)
+__host__ __device__ __forceinline__ uint4 philox_vec(const F& f, uint4 w)
 {
     constexpr unsigned opt = 4 / F::iw;
     typename F::T      out[opt * F::ow];

@@ -205,7 +205,7 @@ PoissonCache::~PoissonCache()
 
 rocrand_status PoissonCache::reserve()
 {
-    if(d_base != nullptr)
+    if(d_base != nullptr || m_host)
         return ROCRAND_STATUS_SUCCESS;
     static_assert(sizeof(PoissonEntriesUpload) < 32764 && sizeof(PoissonDoublesUpload) < 32764,
                   "kernel parameters are limited to 32764 bytes");
@@ -229,6 +229,26 @@ rocrand_status PoissonCache::get(double lambda, cudaStream_t stream, bool with_c
         p.huge        = 1;
         p.lambda      = lambda;
         p.sqrt_lambda = std::sqrt(lambda);
+        return ROCRAND_STATUS_SUCCESS;
+    }
+    if(m_host)
+    {
+        if(lambda != m_lambda || h_thr.empty())
+        {
+            build_poisson_table(lambda, h_table);
+            h_thr.resize(h_table.size);
+            for(uint32_t i = 0; i < h_table.size; i++)
+                h_thr[i] = alias_entry(h_table.prob[i], h_table.alias[i]);
+            m_lambda = lambda;
+        }
+        p.huge   = 0;
+        p.prob   = h_table.prob.data();
+        p.thr    = h_thr.data();
+        p.alias  = h_table.alias.data();
+        p.cdf    = h_table.cdf.data();
+        p.size   = h_table.size;
+        p.offset = h_table.offset;
+        p.lambda = lambda;
         return ROCRAND_STATUS_SUCCESS;
     }
     rocrand_status st = reserve();

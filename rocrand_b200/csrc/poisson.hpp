@@ -96,7 +96,13 @@ public:
     // lambda changed.  with_cdf also uploads the cumulative table (used by Sobol).
     rocrand_status get(double lambda, cudaStream_t stream, bool with_cdf, DistParams& p);
 
+    // Host execution: the tables stay in host memory (no device allocation or upload).
+    void set_host() { m_host = true; }
+
 private:
+    bool                            m_host = false;
+    std::vector<unsigned long long> h_thr;
+    HostPoissonTable                h_table;
     double              m_lambda  = 0.0;
     bool                m_has_cdf = false;
     uint32_t            m_size = 0, m_offset = 0;

@@ -20,6 +20,7 @@
 #include "poisson.hpp"
 #include "batch.hpp"
 #include "sobol_dist.cuh"
+#include "host_exec.hpp"
 #include "sobol_tables.hpp"
 
 #include <algorithm>
@@ -134,6 +135,12 @@ class SobolGenerator final : public rocrand_generator_base_type
     using W = std::conditional_t<kIs64, unsigned long long, uint32_t>;
 
 public:
+    bool set_host_execution() override
+    {
+        m_host_exec = true;
+        m_poisson.set_host();
+        return true;
+    }
     rocrand_rng_type type() const override
     {
         if(kIs64)
@@ -151,7 +158,8 @@ public:
                 return st;
             // likewise the device tables every generate call reads (uploaded once per device)
             lr::Table lt;
-            if(sobol_device_vectors(kIs64, kScrambled) == nullptr || !logf_replay_device(lt))
+            if(!m_host_exec
+               && (sobol_device_vectors(kIs64, kScrambled) == nullptr || !logf_replay_device(lt)))
                 return ROCRAND_STATUS_ALLOCATION_FAILED;
             m_current     = static_cast<uint32_t>(m_offset); // 32-bit counter (sobol.hpp:604)
             m_initialized = true;
@@ -232,8 +240,9 @@ public:
         p.offset      = dp.offset;
         p.lambda      = dp.lambda;
         p.sqrt_lambda = dp.sqrt_lambda;
-        if((d == Dist::NORMAL_F32 || d == Dist::LOGNORMAL_F32 || d == Dist::NORMAL_F16
-            || d == Dist::LOGNORMAL_F16)
+        if(!m_host_exec
+           && (d == Dist::NORMAL_F32 || d == Dist::LOGNORMAL_F32 || d == Dist::NORMAL_F16
+               || d == Dist::LOGNORMAL_F16)
            && !logf_replay_device(p.logf))
             return ROCRAND_STATUS_INTERNAL_ERROR;
         switch(d)
@@ -278,6 +287,8 @@ private:
     {
         using T                = typename SobolOut<K, W>::T;
         constexpr unsigned PPT = sizeof(T) >= 4 ? 4u : 16u / sizeof(T);
+        if(m_host_exec)
+            return run_host<K>(data, n, p);
         const W*           vec = static_cast<const W*>(sobol_device_vectors(kIs64, kScrambled));
         if(vec == nullptr)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
@@ -301,6 +312,50 @@ private:
         const size_t smem = K == SobolKind::POISSON ? p.size * sizeof(double) : 0;
         sobol_fill<W, K><<<dim3(static_cast<unsigned>(bx), m_dims), kBlock, smem, m_stream>>>(a);
         return launch_status();
+    }
+
+    // The same output on the host (host generators without a GPU): point i of dimension d is
+    // the XOR of d's direction vectors over the set bits of Gray(i), with i counted from the
+    // 32-bit start as the kernel counts it, and the distribution applied to it.
+    template<SobolKind K>
+    rocrand_status run_host(void* data, size_t n, const SobolParams& p)
+    {
+        using T                     = typename SobolOut<K, W>::T;
+        using I                     = W;
+        constexpr int         B     = 8 * sizeof(W);
+        const SobolTables&    t     = sobol_tables();
+        if(!t.ok)
+            return ROCRAND_STATUS_INTERNAL_ERROR;
+        const W* const vec = reinterpret_cast<const W*>(
+            kIs64 ? static_cast<const void*>(kScrambled ? t.sv64.data() : t.v64.data())
+                  : static_cast<const void*>(kScrambled ? t.sv32.data() : t.v32.data()));
+        const unsigned long long N = n / m_dims;
+        const uint32_t           offset = m_current;
+        host_parallel_for(static_cast<unsigned long long>(m_dims) * N,
+                          [&](unsigned long long b0, unsigned long long b1) {
+            while(b0 < b1)
+            {
+                const unsigned long long dim = b0 / N, p0 = b0 % N;
+                const unsigned long long p1  = std::min<unsigned long long>(N, p0 + (b1 - b0));
+                const W* const v   = vec + dim * B;
+                const W        c   = kScrambled ? vec[dim] : W(0);
+                T* const       row = static_cast<T*>(data) + dim * N;
+                I              i   = static_cast<I>(static_cast<uint32_t>(offset + static_cast<uint32_t>(p0)));
+                W              x   = 0;
+                const I        g   = i ^ (i >> 1);
+                for(int bit = 0; bit < B; bit++)
+                    if((g >> bit) & 1)
+                        x ^= v[bit];
+                for(unsigned long long q = p0; q < p1; q++)
+                {
+                    row[q] = sobol_apply<K, W>(x ^ c, p, p.cdf);
+                    x ^= v[rzb(i)];
+                    i++;
+                }
+                b0 += p1 - p0;
+            }
+        });
+        return ROCRAND_STATUS_SUCCESS;
     }
 
     unsigned long long m_offset      = 0;

@@ -14,48 +14,53 @@ namespace rb200
 
 // rocrand_normal.h:174-194 roc_f_erfinv, every step rounded as written; the logarithm is the
 // host C library's logf (logf_replay.cuh), which the outer cancellation amplifies.
-__device__ __forceinline__ float erfinv_f(float x, const lr::Table& logf_table)
+RB_HD float erfinv_f(float x, const lr::Table& logf_table)
 {
     const float sgn = (x < 0.0f) ? -1.0f : 1.0f;
-    x               = __fmul_rn(__fsub_rn(1.0f, x), __fadd_rn(1.0f, x));
+    x               = ieee::fmul(ieee::fsub(1.0f, x), ieee::fadd(1.0f, x));
+#if defined(__CUDA_ARCH__)
     const float lnx = lr::logf_host(x, logf_table);
+#else
+    (void)logf_table;
+    const float lnx = std::log(x); // the host's own logf (the host path of host generators)
+#endif
     if(isnan(lnx))
         return 1.0f;
     if(isinf(lnx))
         return 0.0f;
-    const float tt1 = __fadd_rn(2.0f / (3.141592653f * 0.147f), __fmul_rn(0.5f, lnx));
-    const float tt2 = __fmul_rn(1.0f / (0.147f), lnx);
-    return sgn * __fsqrt_rn(__fadd_rn(-tt1, __fsqrt_rn(__fsub_rn(__fmul_rn(tt1, tt1), tt2))));
+    const float tt1 = ieee::fadd(2.0f / (3.141592653f * 0.147f), ieee::fmul(0.5f, lnx));
+    const float tt2 = ieee::fmul(1.0f / (0.147f), lnx);
+    return sgn * ieee::fsqrt(ieee::fadd(-tt1, ieee::fsqrt(ieee::fsub(ieee::fmul(tt1, tt1), tt2))));
 }
 
 // normal_distribution(unsigned int) (rocrand_normal.h:228-233); a 64-bit value uses its high word.
-__device__ __forceinline__ float sobol_normal_f(uint32_t hi32, const lr::Table& logf_table)
+RB_HD float sobol_normal_f(uint32_t hi32, const lr::Table& logf_table)
 {
     const float p = u32_to_f32(hi32);
-    return __fmul_rn(RB_SQRT2, erfinv_f(__fsub_rn(__fmul_rn(2.0f, p), 1.0f), logf_table));
+    return ieee::fmul(RB_SQRT2, erfinv_f(ieee::fsub(ieee::fmul(2.0f, p), 1.0f), logf_table));
 }
 
 template<class W>
-__device__ __forceinline__ uint32_t high32(W x)
+RB_HD uint32_t high32(W x)
 {
     return static_cast<uint32_t>(x >> (8 * sizeof(W) - 32));
 }
 
 // uniform_distribution_double over a Sobol value: 2^-32 based for 32-bit, 2^-53 for 64-bit.
 template<class W>
-__device__ __forceinline__ double sobol_u_f64(W x)
+RB_HD double sobol_u_f64(W x)
 {
     if constexpr(sizeof(W) == 4)
         return u32_to_f64(x);
     else
-        return __fma_rn(__ull2double_rn(x >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
+        return ieee::dfma(ieee::ull2d(x >> 11), RB_2POW53_INV_DOUBLE, RB_2POW53_INV_DOUBLE);
 }
 
 template<class W>
-__device__ __forceinline__ double sobol_normal_d(W x)
+RB_HD double sobol_normal_d(W x)
 {
     const double p = sobol_u_f64(x);
-    return __dmul_rn((double)RB_SQRT2, erfinv_d(__dsub_rn(__dmul_rn(2.0, p), 1.0)));
+    return ieee::dmul((double)RB_SQRT2, erfinv_d(ieee::dsub(ieee::dmul(2.0, p), 1.0)));
 }
 
 enum class SobolKind : int
@@ -106,7 +111,7 @@ struct SobolParams
 };
 
 template<SobolKind K, class W>
-__device__ __forceinline__ typename SobolOut<K, W>::T sobol_apply(W x, const SobolParams& p,
+RB_HD typename SobolOut<K, W>::T sobol_apply(W x, const SobolParams& p,
                                                                    const double* cdf)
 {
     constexpr int B = 8 * sizeof(W);
@@ -125,25 +130,25 @@ __device__ __forceinline__ typename SobolOut<K, W>::T sobol_apply(W x, const Sob
     else if constexpr(K == SobolKind::HALF)
         return u16_to_f16(static_cast<uint32_t>(x >> (B - 16)) & 0xffffu);
     else if constexpr(K == SobolKind::NORMAL_F)
-        return __fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x), p.logf), p.std_f));
+        return ieee::fadd(p.mean_f, ieee::fmul(sobol_normal_f(high32(x), p.logf), p.std_f));
     else if constexpr(K == SobolKind::LOGNORMAL_F)
-        return expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x), p.logf))));
+        return ieee::expf_(ieee::fadd(p.mean_f, ieee::fmul(p.std_f, sobol_normal_f(high32(x), p.logf))));
     else if constexpr(K == SobolKind::NORMAL_D)
-        return __dadd_rn(p.mean_d, __dmul_rn(sobol_normal_d(x), p.std_d));
+        return ieee::dadd(p.mean_d, ieee::dmul(sobol_normal_d(x), p.std_d));
     else if constexpr(K == SobolKind::LOGNORMAL_D)
-        return exp(__dadd_rn(p.mean_d, __dmul_rn(p.std_d, sobol_normal_d(x))));
+        return ieee::exp_(ieee::dadd(p.mean_d, ieee::dmul(p.std_d, sobol_normal_d(x))));
     else if constexpr(K == SobolKind::NORMAL_H)
-        return __float2half_rn(__fadd_rn(p.mean_f, __fmul_rn(sobol_normal_f(high32(x), p.logf), p.std_f)));
+        return __float2half_rn(ieee::fadd(p.mean_f, ieee::fmul(sobol_normal_f(high32(x), p.logf), p.std_f)));
     else if constexpr(K == SobolKind::LOGNORMAL_H)
-        return __float2half_rn(expf(__fadd_rn(p.mean_f, __fmul_rn(p.std_f, sobol_normal_f(high32(x), p.logf)))));
+        return __float2half_rn(ieee::expf_(ieee::fadd(p.mean_f, ieee::fmul(p.std_f, sobol_normal_f(high32(x), p.logf)))));
     else if constexpr(K == SobolKind::POISSON)
     {
         // discrete_cdf (rocrand_discrete.h:92-115): first entry >= x, capped at the last
         double xd;
         if constexpr(sizeof(W) == 4)
-            xd = __dmul_rn(__uint2double_rn(x), RB_2POW32_INV_DOUBLE);
+            xd = ieee::dmul(ieee::u2d(x), RB_2POW32_INV_DOUBLE);
         else
-            xd = __dmul_rn(__ull2double_rn(x), 5.4210108624275221700372640043497e-20);
+            xd = ieee::dmul(ieee::ull2d(x), 5.4210108624275221700372640043497e-20);
         uint32_t lo = 0, hi = p.size - 1;
         while(lo != hi)
         {
@@ -159,7 +164,7 @@ __device__ __forceinline__ typename SobolOut<K, W>::T sobol_apply(W x, const Sob
     {
         static_assert(K == SobolKind::POISSON_HUGE, "kind");
         const double nd = sobol_normal_d(x);
-        return (uint32_t)(long long)round(__dadd_rn(__dmul_rn(p.sqrt_lambda, nd), p.lambda));
+        return (uint32_t)(long long)round(ieee::dadd(ieee::dmul(p.sqrt_lambda, nd), p.lambda));
     }
 }
 
@@ -167,13 +172,25 @@ __device__ __forceinline__ typename SobolOut<K, W>::T sobol_apply(W x, const Sob
 // last value) gives 0, as the reference's device engine does (rocrand_sobol32.h:161-166),
 // which also keeps the table index in range.
 template<class W>
-__device__ __forceinline__ uint32_t rzb(W x)
+RB_HD uint32_t rzb(W x)
 {
     int z;
     if constexpr(sizeof(W) == 4)
+    {
+#if defined(__CUDA_ARCH__)
         z = __ffs(~x);
+#else
+        z = __builtin_ffs(static_cast<int>(~x));
+#endif
+    }
     else
+    {
+#if defined(__CUDA_ARCH__)
         z = __ffsll(static_cast<long long>(~x));
+#else
+        z = __builtin_ffsll(static_cast<long long>(~x));
+#endif
+    }
     return z ? static_cast<uint32_t>(z - 1) : 0u;
 }
 

@@ -15,16 +15,18 @@
 #include "common.hpp"
 #include "dist.cuh"
 #include "generators.hpp"
+#include "host_exec.hpp"
 #include "launch.cuh"
 #include "poisson.hpp"
 
+#include <cstring>
 #include <type_traits>
 
 namespace rb200
 {
 
 template<class W>
-__device__ __forceinline__ W rotl(W x, int d)
+__host__ __device__ __forceinline__ W rotl(W x, int d)
 {
     constexpr int B = 8 * sizeof(W);
     return (x << (d & (B - 1))) | (x >> ((B - d) & (B - 1)));
@@ -80,7 +82,7 @@ TfKeys<W, D> threefry_keys(const W (&key)[D])
 }
 
 template<class W, int D>
-__device__ __forceinline__ TfBlock<W, D> threefry_block(TfBlock<W, D> x, const TfKeys<W, D>& k)
+__host__ __device__ __forceinline__ TfBlock<W, D> threefry_block(TfBlock<W, D> x, const TfKeys<W, D>& k)
 {
 #pragma unroll
     for(int i = 0; i < D; i++)
@@ -179,7 +181,7 @@ struct TfPos
 
 // Words s..s+D-1 of the concatenation (a, b): the engine's interleave.
 template<class W, int D>
-__device__ __forceinline__ TfBlock<W, D> tf_interleave(const TfBlock<W, D>& a, const TfBlock<W, D>& b,
+__host__ __device__ __forceinline__ TfBlock<W, D> tf_interleave(const TfBlock<W, D>& a, const TfBlock<W, D>& b,
                                                        uint32_t s)
 {
     TfBlock<W, D> m;
@@ -215,7 +217,7 @@ struct TfCall
 };
 
 template<class W, int D>
-__device__ __forceinline__ W tf_word(const TfCall<W, D>& a, unsigned long long p)
+__host__ __device__ __forceinline__ W tf_word(const TfCall<W, D>& a, unsigned long long p)
 {
     const unsigned long long q = a.s0 + p;
     const TfBlock<W, D>      b = threefry_block(tf_add(a.c0, q / D), a.keys);
@@ -228,7 +230,7 @@ __device__ __forceinline__ W tf_word(const TfCall<W, D>& a, unsigned long long p
 }
 
 template<class W, int D, class F>
-__device__ void tf_scalar_run(const TfCall<W, D>& a, const F& f, unsigned long long pos,
+__host__ __device__ void tf_scalar_run(const TfCall<W, D>& a, const F& f, unsigned long long pos,
                               typename F::T* out, uint32_t count)
 {
     typename F::T v[F::ow];
@@ -310,6 +312,38 @@ __global__ void __launch_bounds__(kBlock) threefry_fill(TfCall<W, D> a, F f)
     }
 }
 
+// The same output contract on the host (host generators without a GPU): every vector by the
+// general rule of threefry_fill, the head and tail by the same sequential run.
+template<class W, int D, class F>
+static void threefry_run_host(const TfCall<W, D>& a, const F& f)
+{
+    constexpr unsigned opt = D / F::iw;
+    constexpr unsigned VB  = opt * F::ow * sizeof(typename F::T);
+    host_parallel_for(a.vec_n, [&](unsigned long long j0, unsigned long long j1) {
+        for(unsigned long long j = j0; j < j1; j++)
+        {
+            const unsigned long long q = a.s0 + ((j & (kPhiloxRefStride - 1)) == 0 ? a.start0 : a.adj) + D * j;
+            const TfBlock<W, D>      c = tf_add(a.c0, q / D);
+            const uint32_t           s = static_cast<uint32_t>(q % D);
+            TfBlock<W, D>            b = threefry_block(c, a.keys);
+            if(s != 0)
+                b = tf_interleave(b, threefry_block(tf_add(c, 1), a.keys), s);
+            typename F::T out[opt * F::ow];
+            for(unsigned k = 0; k < opt; k++)
+                f(b.w + k * F::iw, out + k * F::ow);
+            std::memcpy(a.vec + j * VB, out, VB);
+        }
+    });
+    using T = typename F::T;
+    if(a.head > 0)
+        tf_scalar_run(a, f, 0, reinterpret_cast<T*>(a.data), a.head);
+    if(a.tail > 0)
+    {
+        const unsigned long long pos = D * a.vec_n + ((a.vec_n % kPhiloxRefStride) == 0 ? a.start0 : a.adj);
+        tf_scalar_run(a, f, pos, reinterpret_cast<T*>(a.data) + (a.n - a.tail), a.tail);
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 
 template<class W, int D, rocrand_rng_type kType>
@@ -317,6 +351,7 @@ class ThreefryGenerator final : public PseudoGeneratorBase
 {
 public:
     rocrand_rng_type type() const override { return kType; }
+    bool             set_host_execution() override { return enable_host(); }
 
     // Output `index` of distribution d comes from engine word index * iw / ow (index a
     // multiple of ow, output aligned to the distribution's vector): that offset.
@@ -464,6 +499,12 @@ private:
         a.vec    = a.data + mis * tsize;
         if(n == 0)
             return ROCRAND_STATUS_SUCCESS;
+        if(m_host_exec)
+        {
+            threefry_run_host(a, f);
+            m_pos.advance(static_cast<unsigned long long>((n + ow - 1) / ow) * iw);
+            return ROCRAND_STATUS_SUCCESS;
+        }
         const size_t             smem    = table_smem_bytes(f);
         const bool               aligned = a.start0 == a.adj && ((a.s0 + a.adj) % D) == 0;
         const unsigned long long work    = a.vec_n > 0 ? a.vec_n : 1;

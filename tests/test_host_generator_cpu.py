@@ -1,0 +1,110 @@
+"""Host generators computed on the CPU (no GPU needed), against the oracle.
+
+In a process without a CUDA device -- or with ROCRAND_B200_HOST_CPU=1, set here so that the
+same test also runs the CPU form on a machine with a GPU -- rocrand_create_generator_host
+returns the generator in host execution: every generate call writes host memory through the
+same engine, output-order and distribution code as the kernels, compiled for the host, with
+the C library's fp32 transcendentals (the reference's host path takes the same ones).  Each
+call of a random sequence of distributions, sizes and misalignments must equal the oracle's
+-- bit for bit, fp32 normals included; fp64 normals within the parity tests' tolerance
+(tests/gpu_util.compare_call).
+"""
+
+import ctypes
+import os
+import zlib
+
+import numpy as np
+import pytest
+
+from oracle import pyorc
+from tests import gpu_util as gu
+
+os.environ["ROCRAND_B200_HOST_CPU"] = "1"
+
+CPU_FAMILIES = {"philox": 404, "threefry2x32": 408, "threefry2x64": 409, "threefry4x32": 410,
+                "threefry4x64": 411}
+DISTS = [("uint", []), ("char", []), ("short", []), ("uniform", []), ("uniform_double", []),
+         ("uniform_half", []), ("normal", [0.0, 1.0]), ("normal", [1.5, 2.0]), ("normal_double", [0.0, 1.0]),
+         ("normal_half", [0.0, 1.0]), ("log_normal", [0.0, 0.5]), ("log_normal_double", [0.0, 0.5]),
+         ("poisson", [0.5]), ("poisson", [10.0]), ("poisson", [1000.0]), ("poisson", [4500.0]),
+         ("ulonglong", [])]
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return pyorc.CLib("orc")
+
+
+def host_generate(lib, g, dist, n, params, mis):
+    """One call into host memory placed (mis * itemsize) bytes past a 64-byte boundary (the
+    oracle's placement); (status, values)."""
+    suffix, dt, _ = pyorc.DISTS[dist]
+    isz = np.dtype(dt).itemsize
+    buf = np.zeros(n + 64 // isz + 16, dtype=dt)
+    base = (-buf.ctypes.data // isz) % (64 // isz)
+    view = buf[base + mis:base + mis + n]
+    st = getattr(lib, "rocrand_" + suffix)(g, ctypes.c_void_p(view.ctypes.data), ctypes.c_size_t(n),
+                                           *pyorc.dist_args(dist, params))
+    return st, view.copy()
+
+
+def run_case(lib, orc, rng, seed, offset, calls, dims=None):
+    g = ctypes.c_void_p()
+    assert lib.rocrand_create_generator_host(ctypes.byref(g), rng) == 0
+    try:
+        if seed is not None:
+            assert lib.rocrand_set_seed(g, seed) == 0
+        if dims is not None:
+            assert lib.rocrand_set_quasi_random_generator_dimensions(g, dims) == 0
+        if offset is not None:
+            assert lib.rocrand_set_offset(g, offset) == 0
+        ref = pyorc.run_sequence(orc, rng, seed, offset, calls, dims=dims)
+        for k, ((d, n, p, mis), (ost, ovals)) in enumerate(zip(calls, ref)):
+            st, vals = host_generate(lib, g, d, n, p, mis)
+            assert st == ost, (rng, d, st, ost)
+            if st != 0:
+                continue
+            if d in gu.BIT_EXACT or d in ("normal", "normal_half", "log_normal"):
+                # fp32 transforms take the C library's functions on the host: bit-exact
+                assert np.array_equal(vals.view(np.uint8), ovals.view(np.uint8)), (rng, d, n, mis)
+            else:
+                gu.compare_call(orc, rng, seed, offset, dims, calls, k, vals, ovals)
+    finally:
+        lib.rocrand_destroy_generator(g)
+
+
+@pytest.mark.parametrize("name", sorted(CPU_FAMILIES))
+def test_cpu_host_generator_sequences(lib, orc, name):
+    rng = CPU_FAMILIES[name]
+    rs = np.random.default_rng(zlib.crc32(name.encode()))
+    seed = int(rs.integers(0, 2**63))
+    offset = int(rs.integers(0, 2**20)) if rs.random() < 0.5 else None
+    calls = []
+    for k in range(24):
+        d, p = DISTS[int(rs.integers(0, len(DISTS)))]
+        n = int(rs.choice([int(rs.integers(1, 40)), int(rs.integers(1, 5000)), int(rs.integers(1, 300000))]))
+        calls.append((d, n, p, int(rs.integers(0, 16))))
+    run_case(lib, orc, rng, seed, offset, calls)
+
+
+QUASI = {"sobol32": 501, "scrambled_sobol32": 502, "sobol64": 504, "scrambled_sobol64": 505}
+
+
+@pytest.mark.parametrize("name", sorted(QUASI))
+def test_cpu_quasi_host_generator_sequences(lib, orc, name):
+    rng = QUASI[name]
+    rs = np.random.default_rng(zlib.crc32(name.encode()))
+    dims = int(rs.choice([1, 3, 64]))
+    offset = int(rs.integers(0, 2**20))
+    calls = []
+    for k in range(16):
+        d, p = DISTS[int(rs.integers(0, len(DISTS)))]
+        n = dims * int(rs.choice([int(rs.integers(1, 40)), int(rs.integers(1, 3000)), int(rs.integers(1, 60000))]))
+        calls.append((d, n, p, int(rs.integers(0, 16))))
+    run_case(lib, orc, rng, None, offset, calls, dims=dims)
+
+
+def test_cpu_host_generator_large_call(lib, orc):
+    """2^22 values in one call (spread over the host's cores) equal the oracle."""
+    run_case(lib, orc, 404, 0xdeadbeef, 0, [("uniform", (1 << 22) + 3, [], 1), ("poisson", 1 << 21, [7.5], 0)])
