@@ -12,12 +12,12 @@ namespace rb200
 {
 
 // f(begin, end) over [0, n) in contiguous chunks, one per host thread (one chunk when n is
-// small).
+// below `grain`: positions cheap enough that threads would cost more than they save).
 template<class F>
-void host_parallel_for(unsigned long long n, F&& f)
+void host_parallel_for(unsigned long long n, F&& f, unsigned long long grain = 1ull << 15)
 {
     const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
-    if(n < (1ull << 15) || hw == 1)
+    if(n < grain || hw == 1)
     {
         f(0ull, n);
         return;

@@ -25,6 +25,7 @@
 #include "common.hpp"
 #include "dist.cuh"
 #include "generators.hpp"
+#include "host_exec.hpp"
 #include "launch.cuh"
 
 #include <cuda_runtime.h>
@@ -59,7 +60,7 @@ __host__ __device__ __forceinline__ uint32_t mt_mix(uint32_t a, uint32_t b, uint
     return m ^ (y >> 1) ^ ((0u - (y & 1u)) & 0x9908b0dfu);
 }
 
-__device__ __forceinline__ uint32_t mt_temper(uint32_t y)
+__host__ __device__ __forceinline__ uint32_t mt_temper(uint32_t y)
 {
     y ^= y >> 11;
     y ^= (y << 7) & 0x9d2c5680u;
@@ -510,10 +511,152 @@ const uint32_t* device_jump_polys()
     return ptr[dev];
 }
 
+// ---- CPU path of the host generators: the same output order on the host's cores ----
+
+// State word held by slot `slot` of lane `lane` (the inverse of word_home).
+inline unsigned slot_word(unsigned lane, unsigned slot)
+{
+    constexpr unsigned kSingle[8] = {0, 113, 170, 283, 340, 397, 510, 567};
+    constexpr unsigned kGroup[11] = {1, 57, 114, 171, 227, 284, 341, 398, 454, 511, 568};
+    if(slot == 0)
+        return kSingle[lane];
+    return kGroup[(slot - 1) / 7] + 7 * lane + (slot - 1) % 7;
+}
+
+// The sequential recurrence in place: word i reads word i + 1 and word i + 397 (mod 624),
+// the later ones already new -- the order mt_twist follows across its lanes.
+inline void mt_twist_host(uint32_t* s)
+{
+    for(unsigned i = 0; i < kMtN; i++)
+        s[i] = mt_mix(s[i], s[(i + 1) % kMtN], s[(i + kMtM) % kMtN]);
+}
+
+// x[0..623] extended to kMtSeq words (the host form of extend_sequence).
+inline void mt_sequence_host(const uint32_t* state, uint32_t* x)
+{
+    std::memcpy(x, state, sizeof(uint32_t) * kMtN);
+    for(unsigned k = kMtN; k < kMtSeq; k++)
+        x[k] = mt_mix(x[k - kMtN], x[k - kMtN + 1], x[k - (kMtN - kMtM)]);
+}
+
+// out[k] = XOR of x[i + k] over the set coefficients i of `poly` (apply_poly for all 624
+// words at once: one pass over the sequence per coefficient).
+inline void mt_apply_poly_host(const uint32_t* poly, const uint32_t* x, uint32_t* out)
+{
+    std::memset(out, 0, sizeof(uint32_t) * kMtN);
+    for(unsigned w = 0; w < kMtN; w++)
+    {
+        for(uint32_t bits = poly[w]; bits; bits &= bits - 1)
+        {
+            const uint32_t* src = x + 32 * w + static_cast<unsigned>(__builtin_ctz(bits));
+            for(unsigned k = 0; k < kMtN; k++)
+                out[k] ^= src[k];
+        }
+    }
+}
+
+// Start states of the 8192 generators, word k of generator e at states[e * 624 + k]: the
+// same two radix-256 jump digits as mt_jump_low and mt_jump_high.
+inline void mt_init_host(const uint32_t* seed_state, uint32_t* states)
+{
+    const uint32_t*       polys = rb200_mt19937_jump_begin;
+    std::vector<uint32_t> x0(kMtSeq);
+    mt_sequence_host(seed_state, x0.data());
+    std::vector<uint32_t> low(static_cast<size_t>(256) * kMtN);
+    std::memcpy(low.data(), seed_state, sizeof(uint32_t) * kMtN);
+    host_parallel_for(
+        255,
+        [&](unsigned long long b, unsigned long long e) {
+            for(unsigned long long e0 = b + 1; e0 <= e; e0++)
+                mt_apply_poly_host(polys + (e0 - 1) * kMtN, x0.data(), low.data() + e0 * kMtN);
+        },
+        2);
+    host_parallel_for(
+        kMtGens,
+        [&](unsigned long long b, unsigned long long e) {
+            std::vector<uint32_t> y(kMtSeq);
+            for(unsigned long long g = b; g < e; g++)
+            {
+                const uint32_t* src = low.data() + (g % 256) * kMtN;
+                const unsigned  e1  = static_cast<unsigned>(g / 256);
+                if(e1 == 0)
+                {
+                    std::memcpy(states + g * kMtN, src, sizeof(uint32_t) * kMtN);
+                    continue;
+                }
+                mt_sequence_host(src, y.data());
+                mt_apply_poly_host(polys + static_cast<size_t>(255 + e1 - 1) * kMtN, y.data(),
+                                   states + g * kMtN);
+            }
+        },
+        2);
+}
+
+// mt_fill on the host: generator g runs its eight lanes' slot groups round by round, with
+// mt_fill's unit numbering, skipping and extra unit; generators are independent.
+template<class F>
+void mt_fill_host(const MtArgs& a, const F& f, uint32_t* states)
+{
+    using T                = typename F::T;
+    constexpr unsigned iw  = F::iw;
+    constexpr unsigned ow  = F::ow;
+    constexpr unsigned per = kMtSlots / iw;
+    constexpr unsigned VB  = sizeof(T) * ow;
+    host_parallel_for(
+        kMtGens,
+        [&](unsigned long long g0, unsigned long long g1) {
+            for(unsigned long long g = g0; g < g1; g++)
+            {
+                uint32_t* s = states + g * kMtN;
+                for(uint32_t rho = 0; rho < a.rounds; rho++)
+                {
+                    if(rho > 0 || a.twist_first)
+                        mt_twist_host(s);
+                    const long long base = static_cast<long long>(rho) * a.full - a.start;
+                    for(unsigned lane = 0; lane < 8; lane++)
+                    {
+                        const long long tid = static_cast<long long>(g * 8 + lane);
+                        for(unsigned G = 0; G < per; G++)
+                        {
+                            const long long q = base + tid + static_cast<long long>(G) * kMtThreads;
+                            if(q < 0 || static_cast<unsigned long long>(q) >= a.total)
+                                continue;
+                            uint32_t in[iw];
+                            for(unsigned i = 0; i < iw; i++)
+                                in[i] = mt_temper(s[slot_word(lane, G * iw + i)]);
+                            T out[ow];
+                            f(in, out);
+                            if(static_cast<unsigned long long>(q) < a.vec_n)
+                            {
+                                std::memcpy(a.vec + static_cast<unsigned long long>(q) * VB, out, VB);
+                                continue;
+                            }
+                            T* data = reinterpret_cast<T*>(a.data);
+                            for(unsigned o = 0; o < ow; o++)
+                            {
+                                if(o < a.head)
+                                    data[o] = out[o];
+                                if(static_cast<int>(o) > static_cast<int>(ow) - static_cast<int>(a.tail) - 1)
+                                    data[a.n + (ow - a.tail - 1) - o] = out[o];
+                            }
+                        }
+                    }
+                }
+            }
+        },
+        64);
+}
+
 class Mt19937Generator final : public PseudoGeneratorBase
 {
 public:
-    ~Mt19937Generator() override { cudaFree(m_arena); }
+    ~Mt19937Generator() override
+    {
+        if(m_arena != nullptr)
+            cudaFree(m_arena);
+    }
+
+    bool set_host_execution() override { return enable_host(); }
 
     rocrand_rng_type type() const override { return ROCRAND_RNG_PSEUDO_MT19937; }
 
@@ -547,6 +690,22 @@ public:
         // that a generate call recorded by a stream capture allocates nothing
         if(m_poisson.reserve() != ROCRAND_STATUS_SUCCESS)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
+        if(m_host_exec)
+        {
+            if(static_cast<size_t>(rb200_mt19937_jump_end - rb200_mt19937_jump_begin)
+               != static_cast<size_t>(kMtPolys) * kMtN)
+                return ROCRAND_STATUS_INTERNAL_ERROR;
+            uint32_t s[kMtN];
+            s[0] = static_cast<uint32_t>((m_seed >> 32) ^ m_seed);
+            for(uint32_t i = 1; i < kMtN; i++)
+                s[i] = 1812433253u * (s[i - 1] ^ (s[i - 1] >> 30)) + i;
+            m_hstate.assign(static_cast<size_t>(kMtGens) * kMtN, 0u);
+            mt_init_host(s, m_hstate.data());
+            m_start       = 0;
+            m_prev_iw     = 0;
+            m_initialized = true;
+            return ROCRAND_STATUS_SUCCESS;
+        }
         const uint32_t* polys = device_jump_polys();
         if(polys == nullptr)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
@@ -652,7 +811,11 @@ private:
         a.twist_first = m_start == 0 ? 1u : 0u;
         a.rounds      = a.total == 0 ? 0u
                                      : static_cast<uint32_t>((m_start + a.total - 1) / full + 1);
-        if(a.total > 0)
+        if(a.total > 0 && m_host_exec)
+        {
+            mt_fill_host(a, f, m_hstate.data());
+        }
+        else if(a.total > 0)
         {
             const size_t smem = mt_fill_smem(f);
             mt_fill<F><<<kMtThreads / kMtBlock, kMtBlock, smem, m_stream>>>(a, f);
@@ -668,6 +831,8 @@ private:
     uint32_t* m_arena   = nullptr;
     uint32_t  m_start   = 0;
     uint32_t  m_prev_iw = 0;
+    // generator states of the CPU path, in word order (generator e at [e * 624])
+    std::vector<uint32_t> m_hstate;
 };
 
 } // namespace

@@ -19,6 +19,7 @@
 #include "common.hpp"
 #include "dist.cuh"
 #include "generators.hpp"
+#include "host_exec.hpp"
 #include "launch.cuh"
 #include "stateful_engines.cuh"
 
@@ -136,6 +137,89 @@ __global__ void __launch_bounds__(kMtgpBlock) mtgp_fill(MtgpArgs a, F fw)
         a.offsets[b] = k;
 }
 
+// mtgp_fill on the host (CPU path of the host generators): generator b's 256 threads take
+// each block step in thread order -- a step's reads end before its first written word, so
+// the order within a step does not change a value -- then every thread applies the
+// distribution to its inputs and writes by mtgp_fill's rules.  Generators are independent.
+template<class F>
+void mtgp_fill_host(const MtgpArgs& a, const F& f)
+{
+    using T                      = typename F::T;
+    constexpr unsigned iw        = F::iw;
+    constexpr unsigned ow        = F::ow;
+    constexpr unsigned VB        = ow * sizeof(T);
+    const unsigned long long str = static_cast<unsigned long long>(kMtgpGens) * kMtgpBlock;
+    host_parallel_for(
+        kMtgpGens,
+        [&](unsigned long long b0, unsigned long long b1) {
+            std::vector<uint32_t> vals(static_cast<size_t>(iw) * kMtgpBlock);
+            std::vector<T>        outs(static_cast<size_t>(ow) * kMtgpBlock);
+            for(unsigned long long b = b0; b < b1; b++)
+            {
+                uint32_t*       s    = a.rings + b * kMtgpState;
+                const uint32_t* p    = a.params + b * kMtgpWords;
+                const int       pos  = static_cast<int>(p[0]);
+                const uint32_t  sh1 = p[1], sh2 = p[2], mask = p[35];
+                const uint32_t* tbl  = p + 3;
+                const uint32_t* tmp  = p + 19;
+                int             k    = a.offsets[b];
+                // iw block steps, then the distribution on each thread's inputs
+                auto gen = [&]() {
+                    for(unsigned i = 0; i < iw; i++)
+                    {
+                        for(uint32_t t = 0; t < kMtgpBlock; t++)
+                        {
+                            uint32_t x = (s[(k + t) & kMtgpMask] & mask) ^ s[(k + t + 1) & kMtgpMask];
+                            uint32_t y = s[(k + t + pos) & kMtgpMask];
+                            x ^= x << sh1;
+                            y                               = x ^ (y >> sh2);
+                            const uint32_t r                = y ^ tbl[y & 0x0f];
+                            s[(k + t + kMtgpN) & kMtgpMask] = r;
+                            uint32_t tt                     = s[(k + t + pos - 1) & kMtgpMask];
+                            tt ^= tt >> 16;
+                            tt ^= tt >> 8;
+                            vals[t * iw + i] = r ^ tmp[tt & 0x0f];
+                        }
+                        k = (k + kMtgpBlock) & kMtgpMask;
+                    }
+                    for(uint32_t t = 0; t < kMtgpBlock; t++)
+                        f(&vals[t * iw], &outs[t * ow]);
+                };
+                unsigned long long index = b * kMtgpBlock; // thread 0's vector index
+                while(index < a.vec_n_down)
+                {
+                    gen();
+                    std::memcpy(a.vec + index * VB, outs.data(), VB * kMtgpBlock);
+                    index += str;
+                }
+                if(index < a.vec_n_up)
+                {
+                    gen();
+                    for(uint32_t t = 0; t < kMtgpBlock; t++)
+                        if(index + t < a.vec_n)
+                            std::memcpy(a.vec + (index + t) * VB, &outs[t * ow], VB);
+                    index += str;
+                }
+                if(ow > 1 && (a.head > 0 || a.tail > 0))
+                {
+                    gen();
+                    T* data = reinterpret_cast<T*>(a.data);
+                    for(uint32_t t = 0; t < kMtgpBlock; t++)
+                    {
+                        if(index + t == a.vec_n_up)
+                            for(unsigned o = 0; o < a.head; o++)
+                                data[o] = outs[t * ow + o];
+                        if(index + t == a.vec_n_up + 1)
+                            for(unsigned o = 0; o < a.tail; o++)
+                                data[a.n - a.tail + o] = outs[t * ow + o];
+                    }
+                }
+                a.offsets[b] = k;
+            }
+        },
+        2);
+}
+
 // Parameter sets on each device, uploaded once.
 const uint32_t* device_params()
 {
@@ -164,7 +248,13 @@ const uint32_t* device_params()
 class Mtgp32Generator final : public PseudoGeneratorBase
 {
 public:
-    ~Mtgp32Generator() override { cudaFree(m_rings); }
+    ~Mtgp32Generator() override
+    {
+        if(m_rings != nullptr)
+            cudaFree(m_rings);
+    }
+
+    bool set_host_execution() override { return enable_host(); }
 
     rocrand_rng_type type() const override { return ROCRAND_RNG_PSEUDO_MTGP32; }
 
@@ -199,11 +289,16 @@ public:
         // that a generate call recorded by a stream capture allocates nothing
         if(m_poisson.reserve() != ROCRAND_STATUS_SUCCESS)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
-        m_params = device_params();
+        const size_t pbytes = static_cast<size_t>(rb200_mtgp32_params_end - rb200_mtgp32_params_begin);
+        if(pbytes != 12 + sizeof(uint32_t) * kMtgpWords * kMtgpGens
+           || std::memcmp(rb200_mtgp32_params_begin, "RBMTGP01", 8) != 0)
+            return ROCRAND_STATUS_INTERNAL_ERROR;
+        m_params = m_host_exec ? reinterpret_cast<const uint32_t*>(rb200_mtgp32_params_begin + 12)
+                               : device_params();
         if(m_params == nullptr)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
         constexpr size_t kRingWords = static_cast<size_t>(kMtgpGens) * kMtgpState;
-        if(m_rings == nullptr)
+        if(m_rings == nullptr && !m_host_exec)
         {
             if(cudaMalloc(&m_rings, sizeof(uint32_t) * kRingWords + sizeof(int) * kMtgpGens)
                != cudaSuccess)
@@ -230,6 +325,14 @@ public:
             s[1] = hidden;
             for(uint32_t k = 1; k < static_cast<uint32_t>(kMtgpN); k++)
                 s[k] ^= 1812433253u * (s[k - 1] ^ (s[k - 1] >> 30)) + k;
+        }
+        if(m_host_exec)
+        {
+            // the host copy: rings, then the 512 ring offsets
+            m_hrings.assign(kRingWords + kMtgpGens, 0u);
+            std::memcpy(m_hrings.data(), rings.data(), sizeof(uint32_t) * kRingWords);
+            m_initialized = true;
+            return ROCRAND_STATUS_SUCCESS;
         }
         // pageable sources: the copies have read them when cudaMemcpyAsync returns
         if(cudaMemcpyAsync(m_rings, rings.data(), sizeof(uint32_t) * kRingWords,
@@ -277,8 +380,9 @@ private:
         const uintptr_t    addr = reinterpret_cast<uintptr_t>(data);
         const size_t       mis  = (ow - addr / tsize % ow) % ow;
         MtgpArgs           a;
-        a.rings      = m_rings;
-        a.offsets    = reinterpret_cast<int*>(m_rings + static_cast<size_t>(kMtgpGens) * kMtgpState);
+        uint32_t*          rings = m_host_exec ? m_hrings.data() : m_rings;
+        a.rings      = rings;
+        a.offsets    = reinterpret_cast<int*>(rings + static_cast<size_t>(kMtgpGens) * kMtgpState);
         a.params     = m_params;
         a.head       = static_cast<uint32_t>(n < mis ? n : mis);
         a.tail       = static_cast<uint32_t>((n - a.head) % ow);
@@ -290,6 +394,11 @@ private:
         a.vec_n_down = a.vec_n - rem;
         a.vec_n_up   = rem == 0 ? a.vec_n_down : a.vec_n_down + kMtgpBlock;
         // every call steps every generator (mtgp32.hpp:268-305), even with nothing to write
+        if(m_host_exec)
+        {
+            mtgp_fill_host(a, f);
+            return ROCRAND_STATUS_SUCCESS;
+        }
         const size_t smem = table_smem_bytes(f);
         mtgp_fill<F><<<kMtgpGens, kMtgpBlock, smem, m_stream>>>(a, f);
         return launch_status();
@@ -297,6 +406,8 @@ private:
 
     uint32_t*       m_rings  = nullptr;
     const uint32_t* m_params = nullptr;
+    // rings and offsets of the CPU path (the device layout, in host memory)
+    std::vector<uint32_t> m_hrings;
 };
 
 } // namespace

@@ -22,13 +22,16 @@
 #include "common.hpp"
 #include "dist.cuh"
 #include "generators.hpp"
+#include "host_exec.hpp"
 #include "jump_tables.hpp"
 #include "launch.cuh"
 #include "poisson.hpp"
 #include "stateful_engines.cuh"
 #include "batch.hpp"
 
+#include <algorithm>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <type_traits>
 #include <vector>
@@ -48,6 +51,37 @@ struct InitArgs
     uint32_t* arena;
 };
 
+// x <- J^e x from the per-digit tables: one matrix per non-zero base-4 digit of e (GF(2)
+// engines; the device init kernel and the CPU path share it).
+template<int NJ>
+__host__ __device__ __forceinline__ void gf2_jump_digits(const uint32_t* tables, uint32_t e, uint32_t* x)
+{
+    constexpr size_t msize = static_cast<size_t>(NJ) * 32 * NJ;
+    for(int p = 0; p < kJumpDigits; p++)
+    {
+        const uint32_t d = (e >> (2 * p)) & 3u;
+        if(d)
+            gf2_apply<NJ>(tables + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
+    }
+}
+
+// The same for the MRG engines: each digit matrix is a pair (component 1 mod m1, component
+// 2 mod m2) of 3 x 3 matrices.
+__host__ __device__ __forceinline__ void mod_jump_digits(const uint64_t* tables, uint64_t m1, uint64_t m2,
+                                                         uint32_t e, uint32_t* x)
+{
+    for(int p = 0; p < kJumpDigits; p++)
+    {
+        const uint32_t d = (e >> (2 * p)) & 3u;
+        if(d)
+        {
+            const uint64_t* t = tables + ((static_cast<size_t>(p) * 3 + (d - 1)) * 2) * 9;
+            mod_apply(t, m1, x);
+            mod_apply(t + 9, m2, x + 3);
+        }
+    }
+}
+
 // GF(2) engines (XORWOW: 5 jump words + the Weyl counter copied; LFSR113: 4 words).
 template<int NJ, int NW>
 __global__ void __launch_bounds__(kBlock) init_gf2(InitArgs a, const uint32_t* __restrict__ tables)
@@ -60,13 +94,7 @@ __global__ void __launch_bounds__(kBlock) init_gf2(InitArgs a, const uint32_t* _
 #pragma unroll
     for(int k = 0; k < NW; k++)
         x[k] = a.base[which][k];
-    constexpr size_t msize = static_cast<size_t>(NJ) * 32 * NJ;
-    for(int p = 0; p < kJumpDigits; p++)
-    {
-        const uint32_t d = (e >> (2 * p)) & 3u;
-        if(d)
-            gf2_apply<NJ>(tables + (static_cast<size_t>(p) * 3 + (d - 1)) * msize, x);
-    }
+    gf2_jump_digits<NJ>(tables, e, x);
 #pragma unroll
     for(int k = 0; k < NW; k++)
         a.arena[static_cast<size_t>(k) * kE + e] = x[k];
@@ -125,16 +153,7 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
     for(int k = 0; k < 6; k++)
         x[k] = a.base[which][k];
-    for(int p = 0; p < kJumpDigits; p++)
-    {
-        const uint32_t d = (e >> (2 * p)) & 3u;
-        if(d)
-        {
-            const uint64_t* t = tables + ((static_cast<size_t>(p) * 3 + (d - 1)) * 2) * 9;
-            mod_apply(t, m1, x);
-            mod_apply(t + 9, m2, x + 3);
-        }
-    }
+    mod_jump_digits(tables, m1, m2, e, x);
 #pragma unroll
     for(int k = 0; k < 6; k++)
         a.arena[static_cast<size_t>(k) * kE + e] = x[k];
@@ -211,6 +230,70 @@ __global__ void __launch_bounds__(kBlock) stateful_fill(FillArgs a, F f)
         a.arena[static_cast<size_t>(k) * kE + e] = eng.w[k];
 }
 
+// The same output contract on the host (host generators without a GPU): slot t runs
+// stateful_fill's body for its engine; slots are independent (distinct engines, distinct
+// output vectors, the head and tail written by one slot), so they spread over the host's
+// cores.
+template<class E, class F>
+static void stateful_slot_host(const FillArgs& a, const F& f, uint32_t t)
+{
+    const bool loops = t < a.vec_n;
+    const bool edges = F::ow > 1 && (a.head > 0 || a.tail > 0) && (a.vec_n % kE) == t;
+    if(!loops && !edges)
+        return;
+    const uint32_t e = (t + a.start) & (kE - 1);
+    E              eng;
+    for(int k = 0; k < E::kWords; k++)
+        eng.w[k] = a.arena[static_cast<size_t>(k) * kE + e];
+    using T = typename F::T;
+    constexpr unsigned VB = F::ow * sizeof(T);
+    uint32_t           in[F::iw];
+    T                  out[F::ow];
+    unsigned long long j = t;
+    for(; j < a.vec_n; j += kE)
+    {
+        for(unsigned i = 0; i < F::iw; i++)
+            in[i] = eng.next();
+        f(in, out);
+        store_small(a.vec + j * VB, out);
+    }
+    if(F::ow > 1 && j == a.vec_n)
+    {
+        T* data = reinterpret_cast<T*>(a.data);
+        if(a.head > 0)
+        {
+            for(unsigned i = 0; i < F::iw; i++)
+                in[i] = eng.next();
+            f(in, out);
+            for(unsigned o = 0; o < a.head; o++)
+                data[o] = out[o];
+        }
+        if(a.tail > 0)
+        {
+            for(unsigned i = 0; i < F::iw; i++)
+                in[i] = eng.next();
+            f(in, out);
+            for(unsigned o = 0; o < a.tail; o++)
+                data[a.n - a.tail + o] = out[o];
+        }
+    }
+    for(int k = 0; k < E::kWords; k++)
+        a.arena[static_cast<size_t>(k) * kE + e] = eng.w[k];
+}
+
+template<class E, class F>
+static void stateful_fill_host(const FillArgs& a, const F& f)
+{
+    // slots below min(vec_n, E) loop; the edge slot vec_n % E is among them unless vec_n < E
+    const unsigned long long active = std::min<unsigned long long>(a.vec_n, kE);
+    host_parallel_for(active, [&](unsigned long long t0, unsigned long long t1) {
+        for(unsigned long long t = t0; t < t1; t++)
+            stateful_slot_host<E>(a, f, static_cast<uint32_t>(t));
+    });
+    if(a.vec_n < kE)
+        stateful_slot_host<E>(a, f, static_cast<uint32_t>(a.vec_n));
+}
+
 // ---------------------------------------------------------------------------------------
 // Host side: seeding, base states and tables.
 
@@ -223,6 +306,36 @@ struct DeviceTables
     std::vector<const void*>   ptr = std::vector<const void*>(64, nullptr);
 };
 
+// Host copies of the per-digit jump tables, computed once per family (the source of the
+// device uploads and the tables of the CPU path).
+struct HostDigitTables
+{
+    std::vector<uint32_t> t32; // GF(2) families
+    std::vector<uint64_t> t64; // MRG families
+};
+
+static const HostDigitTables& host_digit_tables(Family fam)
+{
+    static HostDigitTables t[4];
+    static std::once_flag  once[4];
+    const int              i = static_cast<int>(fam);
+    std::call_once(once[i], [&] {
+        HostDigitTables& h = t[i];
+        switch(fam)
+        {
+            case Family::XORWOW: h.t32 = gf2_digit_tables(gf2_pow2(xorwow_step_matrix(), 67)); break;
+            case Family::LFSR113: h.t32 = gf2_digit_tables(gf2_pow2(lfsr113_step_matrix(), 55)); break;
+            case Family::MRG32K3A:
+                h.t64 = mod_digit_tables(mod_pow2(mrg32k3a_step1(), 76), mod_pow2(mrg32k3a_step2(), 76));
+                break;
+            case Family::MRG31K3P:
+                h.t64 = mod_digit_tables(mod_pow2(mrg31k3p_step1(), 72), mod_pow2(mrg31k3p_step2(), 72));
+                break;
+        }
+    });
+    return t[i];
+}
+
 static const void* digit_tables(Family fam)
 {
     static DeviceTables cache[4];
@@ -231,19 +344,8 @@ static const void* digit_tables(Family fam)
     std::lock_guard<std::mutex> lock(c.mu);
     if(c.ptr[dev])
         return c.ptr[dev];
-    std::vector<uint32_t> t32;
-    std::vector<uint64_t> t64;
-    switch(fam)
-    {
-        case Family::XORWOW: t32 = gf2_digit_tables(gf2_pow2(xorwow_step_matrix(), 67)); break;
-        case Family::LFSR113: t32 = gf2_digit_tables(gf2_pow2(lfsr113_step_matrix(), 55)); break;
-        case Family::MRG32K3A:
-            t64 = mod_digit_tables(mod_pow2(mrg32k3a_step1(), 76), mod_pow2(mrg32k3a_step2(), 76));
-            break;
-        case Family::MRG31K3P:
-            t64 = mod_digit_tables(mod_pow2(mrg31k3p_step1(), 72), mod_pow2(mrg31k3p_step2(), 72));
-            break;
-    }
+    const std::vector<uint32_t>& t32 = host_digit_tables(fam).t32;
+    const std::vector<uint64_t>& t64 = host_digit_tables(fam).t64;
     void*        d     = nullptr;
     const size_t bytes = t32.empty() ? t64.size() * 8 : t32.size() * 4;
     if(cudaMalloc(&d, bytes) != cudaSuccess)
@@ -519,7 +621,13 @@ public:
         if constexpr(kFam == Family::LFSR113)
             m_seed4 = make_uint4(2u, 8u, 16u, 128u); // lfsr113.hpp:178-186
     }
-    ~StatefulGenerator() override { cudaFree(m_arena); }
+    ~StatefulGenerator() override
+    {
+        if(m_arena != nullptr)
+            cudaFree(m_arena);
+    }
+
+    bool set_host_execution() override { return enable_host(); }
 
     rocrand_rng_type type() const override
     {
@@ -608,7 +716,7 @@ public:
         // that a generate call recorded by a stream capture allocates nothing
         if(m_poisson.reserve() != ROCRAND_STATUS_SUCCESS)
             return ROCRAND_STATUS_ALLOCATION_FAILED;
-        if(m_arena == nullptr)
+        if(m_arena == nullptr && !m_host_exec)
         {
             if(cudaMalloc(&m_arena, sizeof(uint32_t) * 6 * kE) != cudaSuccess)
             {
@@ -629,6 +737,13 @@ public:
         }
         a.start = m_start;
         a.arena = m_arena;
+        if(m_host_exec)
+        {
+            const rocrand_status hs = init_host(a);
+            if(hs == ROCRAND_STATUS_SUCCESS)
+                m_initialized = true;
+            return hs;
+        }
         const unsigned blocks = kE / kBlock;
         if constexpr(kFam == Family::XORWOW)
         {
@@ -743,6 +858,8 @@ public:
         }
         else
         {
+            if(m_host_exec)
+                return ROCRAND_STATUS_TYPE_ERROR; // the batched fill is a device launch
             rocrand_status st = init();
             if(st != ROCRAND_STATUS_SUCCESS)
                 return st;
@@ -778,14 +895,18 @@ private:
         a.n     = n;
         a.data  = static_cast<unsigned char*>(data);
         a.vec   = a.data + mis * tsize;
-        if(n > 0)
+        using Eng = std::conditional_t<
+            kFam == Family::XORWOW, XorwowEngine,
+            std::conditional_t<kFam == Family::LFSR113, Lfsr113Engine,
+                               std::conditional_t<kFam == Family::MRG32K3A, Mrg32k3aEngine, Mrg31k3pEngine>>>;
+        if(n > 0 && m_host_exec)
+        {
+            a.arena = m_harena.data();
+            stateful_fill_host<Eng>(a, f);
+        }
+        else if(n > 0)
         {
             const size_t smem = table_smem_bytes(f);
-            using Eng         = std::conditional_t<
-                kFam == Family::XORWOW, XorwowEngine,
-                std::conditional_t<kFam == Family::LFSR113, Lfsr113Engine,
-                                   std::conditional_t<kFam == Family::MRG32K3A, Mrg32k3aEngine,
-                                                      Mrg31k3pEngine>>>;
             stateful_fill<Eng, F><<<kE / kBlock, kBlock, smem, m_stream>>>(a, f);
             const rocrand_status st = launch_status();
             if(st != ROCRAND_STATUS_SUCCESS)
@@ -795,8 +916,64 @@ private:
         return ROCRAND_STATUS_SUCCESS;
     }
 
+    // Host execution: engine e = J^e base[e < start] on the host's cores, from the same
+    // tables as the device init (the per-digit matrices; XORWOW's jump polynomials).
+    rocrand_status init_host(const InitArgs& a)
+    {
+        m_harena.assign(static_cast<size_t>(6) * kE, 0u);
+        uint32_t* arena = m_harena.data();
+        if constexpr(kFam == Family::XORWOW)
+        {
+            const size_t bytes = static_cast<size_t>(rb200_xorwow_jump_end - rb200_xorwow_jump_begin);
+            if(bytes != sizeof(uint32_t) * 5 * kE)
+                return ROCRAND_STATUS_INTERNAL_ERROR;
+            const uint32_t* polys  = reinterpret_cast<const uint32_t*>(rb200_xorwow_jump_begin);
+            auto            tables = std::make_unique<XorwowJumpTable[]>(2);
+            for(int b = 0; b < 2; b++)
+            {
+                uint32_t seq[kXorwowSeqWords];
+                xorwow_word_sequence(a.base[b], seq);
+                xorwow_build_jump_table(tables[b], seq, 0, 1);
+            }
+            host_parallel_for(kE, [&](unsigned long long e0, unsigned long long e1) {
+                for(unsigned long long e = e0; e < e1; e++)
+                {
+                    const int which = e < a.start ? 1 : 0;
+                    uint32_t  x[5];
+                    xorwow_jump(tables[which], polys, static_cast<uint32_t>(e), x);
+                    for(int w = 0; w < 5; w++)
+                        arena[static_cast<size_t>(w) * kE + e] = x[w];
+                    arena[static_cast<size_t>(5) * kE + e] = a.base[which][5];
+                }
+            });
+        }
+        else
+        {
+            const HostDigitTables& t = host_digit_tables(kFam);
+            host_parallel_for(kE, [&](unsigned long long e0, unsigned long long e1) {
+                for(unsigned long long e = e0; e < e1; e++)
+                {
+                    const int which = e < a.start ? 1 : 0;
+                    uint32_t  x[6];
+                    std::memcpy(x, a.base[which], sizeof(x));
+                    if constexpr(kFam == Family::LFSR113)
+                        gf2_jump_digits<4>(t.t32.data(), static_cast<uint32_t>(e), x);
+                    else if constexpr(kFam == Family::MRG32K3A)
+                        mod_jump_digits(t.t64.data(), 4294967087ull, 4294944443ull, static_cast<uint32_t>(e), x);
+                    else
+                        mod_jump_digits(t.t64.data(), 2147483647ull, 2147462579ull, static_cast<uint32_t>(e), x);
+                    for(int w = 0; w < 6; w++)
+                        arena[static_cast<size_t>(w) * kE + e] = x[w];
+                }
+            });
+        }
+        return ROCRAND_STATUS_SUCCESS;
+    }
+
     uint4     m_seed4 = {0, 0, 0, 0};
     uint32_t* m_arena = nullptr;
+    // engine states of the CPU path (the device arena's layout, in host memory)
+    std::vector<uint32_t> m_harena;
     uint32_t  m_start = 0;
     // rocrand_b200_set_output_position: engines placed after m_pos_vectors vectors of
     // m_pos_values values each (replaces the offset until the next set_offset)

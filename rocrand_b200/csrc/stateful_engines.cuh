@@ -1,6 +1,7 @@
-// stateful_engines.cuh -- device step functions of the XORWOW, MRG32k3a, MRG31k3p and
-// LFSR113 engines, their jump-table application and small vector stores; shared by the
-// per-generator kernels (stateful.cu) and the batched fill (batch.cu).
+// stateful_engines.cuh -- step functions of the XORWOW, MRG32k3a, MRG31k3p and LFSR113
+// engines, their jump-table application and small vector stores; shared by the
+// per-generator kernels (stateful.cu), the batched fill (batch.cu) and the CPU path of the
+// host generators (stateful.cu), which runs the same functions compiled for the host.
 #pragma once
 
 #include "common.hpp"
@@ -10,7 +11,18 @@
 namespace rb200
 {
 
-// ---- engines (device step functions; the state is NW 32-bit words) ----
+// Read-only load: through the non-coherent cache on the device, a plain load on the host.
+template<class T>
+__host__ __device__ __forceinline__ T ld_ro(const T* p)
+{
+#if defined(__CUDA_ARCH__)
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
+// ---- engines (step functions; the state is NW 32-bit words) ----
 
 struct XorwowEngine // rocrand_xorwow.h:165-177
 {
@@ -18,7 +30,7 @@ struct XorwowEngine // rocrand_xorwow.h:165-177
     static constexpr int kGf2    = 5; // words covered by the jump matrices
     static constexpr int kUnroll = 5; // steps after which the state words are back in place
     uint32_t             w[kWords];
-    __device__ __forceinline__ uint32_t next()
+    __host__ __device__ __forceinline__ uint32_t next()
     {
         const uint32_t t = w[0] ^ (w[0] >> 2);
         w[0]             = w[1];
@@ -37,7 +49,7 @@ struct Lfsr113Engine // rocrand_lfsr113.h:146-160
     static constexpr int kGf2    = 4;
     static constexpr int kUnroll = 1;
     uint32_t             w[kWords];
-    __device__ __forceinline__ uint32_t next()
+    __host__ __device__ __forceinline__ uint32_t next()
     {
         uint32_t b;
         b    = ((w[0] << 6) ^ w[0]) >> 13;
@@ -59,23 +71,23 @@ struct Mrg32k3aEngine // rocrand_mrg32k3a.h:160-190: g1[0..2], g2[0..2]
     static constexpr uint64_t kM1 = 4294967087ull, kM2 = 4294944443ull;
     uint32_t                  w[kWords];
     // t < 2 m: t mod m, with the comparison and subtraction on 32-bit words (t - m < 2^32)
-    __device__ __forceinline__ static uint32_t sub_once(uint64_t t, uint32_t m)
+    __host__ __device__ __forceinline__ static uint32_t sub_once(uint64_t t, uint32_t m)
     {
         const uint32_t lo = static_cast<uint32_t>(t);
         return (static_cast<uint32_t>(t >> 32) != 0u || lo >= m) ? lo - m : lo;
     }
     // p < 2^54: 2^32 = 209 (mod m1) folds p below 2^33 < 2 m1
-    __device__ __forceinline__ static uint32_t mod_m1(uint64_t p)
+    __host__ __device__ __forceinline__ static uint32_t mod_m1(uint64_t p)
     {
         return sub_once(209ull * (p >> 32) + (p & 0xffffffffull), static_cast<uint32_t>(kM1));
     }
     // p < 2^54: two folds by 2^32 = 22853 (mod m2) bring p below 2^33 < 2 m2
-    __device__ __forceinline__ static uint32_t mod_m2(uint64_t p)
+    __host__ __device__ __forceinline__ static uint32_t mod_m2(uint64_t p)
     {
         p = 22853ull * (p >> 32) + (p & 0xffffffffull);
         return sub_once(22853ull * (p >> 32) + (p & 0xffffffffull), static_cast<uint32_t>(kM2));
     }
-    __device__ __forceinline__ uint32_t next()
+    __host__ __device__ __forceinline__ uint32_t next()
     {
         const uint32_t p1 = mod_m1(1403580ull * w[1] + 810728ull * static_cast<uint32_t>(static_cast<uint32_t>(kM1) - w[0]));
         w[0] = w[1];
@@ -95,7 +107,7 @@ struct Mrg31k3pEngine // rocrand_mrg31k3p.h:155-185: x1[0..2], x2[0..2]
     static constexpr int      kUnroll = 3;
     static constexpr uint32_t kM1 = 2147483647u, kM2 = 2147462579u;
     uint32_t                  w[kWords];
-    __device__ __forceinline__ uint32_t next()
+    __host__ __device__ __forceinline__ uint32_t next()
     {
         uint32_t t = (((w[1] & 511u) << 22) + (w[1] >> 9)) + (((w[2] & 16777215u) << 7) + (w[2] >> 24));
         t -= (t >= kM1) ? kM1 : 0u;
@@ -122,7 +134,7 @@ struct Mrg31k3pEngine // rocrand_mrg31k3p.h:155-185: x1[0..2], x2[0..2]
 // ---- initialisation: engine e = J^e * base[e < start] ----
 
 template<int N>
-__device__ __forceinline__ void gf2_apply(const uint32_t* __restrict__ m, uint32_t* x)
+__host__ __device__ __forceinline__ void gf2_apply(const uint32_t* __restrict__ m, uint32_t* x)
 {
     uint32_t y[N];
 #pragma unroll
@@ -139,7 +151,7 @@ __device__ __forceinline__ void gf2_apply(const uint32_t* __restrict__ m, uint32
             const uint32_t* row  = m + (i * 32 + b) * N;
 #pragma unroll
             for(int k = 0; k < N; k++)
-                y[k] ^= mask & __ldg(row + k);
+                y[k] ^= mask & ld_ro(row + k);
         }
     }
 #pragma unroll
@@ -147,7 +159,7 @@ __device__ __forceinline__ void gf2_apply(const uint32_t* __restrict__ m, uint32
         x[k] = y[k];
 }
 
-__device__ __forceinline__ void mod_apply(const uint64_t* __restrict__ a, uint64_t m, uint32_t* x)
+__host__ __device__ __forceinline__ void mod_apply(const uint64_t* __restrict__ a, uint64_t m, uint32_t* x)
 {
     uint32_t y[3];
 #pragma unroll
@@ -156,7 +168,7 @@ __device__ __forceinline__ void mod_apply(const uint64_t* __restrict__ a, uint64
         uint64_t s = 0;
 #pragma unroll
         for(int c = 0; c < 3; c++)
-            s += (__ldg(reinterpret_cast<const unsigned long long*>(a) + r * 3 + c) * x[c]) % m;
+            s += (ld_ro(reinterpret_cast<const unsigned long long*>(a) + r * 3 + c) * x[c]) % m;
         y[r] = static_cast<uint32_t>(s % m);
     }
 #pragma unroll
@@ -185,7 +197,7 @@ struct XorwowJumpTable
 
 // Builds the table of one base from its word sequence (any memory space the block can
 // read); called by all `nthreads` threads of the block, which synchronise afterwards.
-__device__ __forceinline__ void xorwow_build_jump_table(XorwowJumpTable& t, const uint32_t* seq,
+__host__ __device__ __forceinline__ void xorwow_build_jump_table(XorwowJumpTable& t, const uint32_t* seq,
                                                         uint32_t tid, uint32_t nthreads)
 {
     for(uint32_t i = tid; i < kXorwowGroups * 16; i += nthreads)
@@ -210,13 +222,13 @@ __device__ __forceinline__ void xorwow_build_jump_table(XorwowJumpTable& t, cons
 
 // x[0..4] <- J^e of the table's base; polys = the build-time table, word-major with stride
 // kStatefulEngines.  The Weyl word is left as it is (a subsequence jump keeps it).
-__device__ __forceinline__ void xorwow_jump(const XorwowJumpTable& t, const uint32_t* __restrict__ polys,
+__host__ __device__ __forceinline__ void xorwow_jump(const XorwowJumpTable& t, const uint32_t* __restrict__ polys,
                                             uint32_t e, uint32_t* x)
 {
     uint32_t c[5];
 #pragma unroll
     for(int j = 0; j < 5; j++)
-        c[j] = __ldg(polys + static_cast<size_t>(j) * kStatefulEngines + e);
+        c[j] = ld_ro(polys + static_cast<size_t>(j) * kStatefulEngines + e);
     uint32_t y0 = 0u, y1 = 0u, y2 = 0u, y3 = 0u, y4 = 0u;
 #pragma unroll
     for(int g = 0; g < kXorwowGroups; g++)
@@ -238,9 +250,12 @@ __device__ __forceinline__ void xorwow_jump(const XorwowJumpTable& t, const uint
 }
 
 template<class T, unsigned N>
-__device__ __forceinline__ void store_small(unsigned char* p, const T (&v)[N])
+__host__ __device__ __forceinline__ void store_small(unsigned char* p, const T (&v)[N])
 {
     constexpr unsigned VB = sizeof(T) * N;
+#if !defined(__CUDA_ARCH__)
+    memcpy(p, v, VB);
+#else
     if constexpr(VB == 4)
     {
         uint32_t w;
@@ -260,6 +275,7 @@ __device__ __forceinline__ void store_small(unsigned char* p, const T (&v)[N])
         memcpy(&w, v, 16);
         __stcs(reinterpret_cast<uint4*>(p), w);
     }
+#endif
 }
 
 } // namespace rb200

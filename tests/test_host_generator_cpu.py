@@ -22,8 +22,10 @@ from tests import gpu_util as gu
 
 os.environ["ROCRAND_B200_HOST_CPU"] = "1"
 
-CPU_FAMILIES = {"philox": 404, "threefry2x32": 408, "threefry2x64": 409, "threefry4x32": 410,
-                "threefry4x64": 411}
+CPU_FAMILIES = {"xorwow": 401, "mrg32k3a": 402, "mtgp32": 403, "philox": 404, "mrg31k3p": 405,
+                "lfsr113": 406, "mt19937": 407, "threefry2x32": 408, "threefry2x64": 409,
+                "threefry4x32": 410, "threefry4x64": 411}
+NO_OFFSET = {403, 407}  # MTGP32 and MT19937 take no offset (mtgp32.hpp:389-393, mt19937.hpp:758-763)
 DISTS = [("uint", []), ("char", []), ("short", []), ("uniform", []), ("uniform_double", []),
          ("uniform_half", []), ("normal", [0.0, 1.0]), ("normal", [1.5, 2.0]), ("normal_double", [0.0, 1.0]),
          ("normal_half", [0.0, 1.0]), ("log_normal", [0.0, 0.5]), ("log_normal_double", [0.0, 0.5]),
@@ -79,7 +81,7 @@ def test_cpu_host_generator_sequences(lib, orc, name):
     rng = CPU_FAMILIES[name]
     rs = np.random.default_rng(zlib.crc32(name.encode()))
     seed = int(rs.integers(0, 2**63))
-    offset = int(rs.integers(0, 2**20)) if rs.random() < 0.5 else None
+    offset = int(rs.integers(0, 2**20)) if rs.random() < 0.5 and rng not in NO_OFFSET else None
     calls = []
     for k in range(24):
         d, p = DISTS[int(rs.integers(0, len(DISTS)))]
@@ -108,3 +110,47 @@ def test_cpu_quasi_host_generator_sequences(lib, orc, name):
 def test_cpu_host_generator_large_call(lib, orc):
     """2^22 values in one call (spread over the host's cores) equal the oracle."""
     run_case(lib, orc, 404, 0xdeadbeef, 0, [("uniform", (1 << 22) + 3, [], 1), ("poisson", 1 << 21, [7.5], 0)])
+
+
+CPU_ONLY_SCRIPT = r"""
+import ctypes, sys
+import numpy as np
+import rocrand_b200
+from oracle import pyorc
+lib = rocrand_b200.load_library()
+orc = pyorc.CLib("orc")
+for rng in (401, 403, 404, 407, 501):
+    calls = [("uint", 1000, [], 0), ("uniform", 777, [], 3), ("poisson", 5000, [12.5], 1)]
+    ref = pyorc.run_sequence(orc, rng, 42 if rng != 501 else None, None, calls)
+    g = ctypes.c_void_p()
+    assert lib.rocrand_create_generator_host(ctypes.byref(g), rng) == 0
+    if rng != 501:
+        assert lib.rocrand_set_seed(g, 42) == 0
+    for (d, n, p, mis), (ost, ovals) in zip(calls, ref):
+        suffix, dt, _ = pyorc.DISTS[d]
+        buf = np.zeros(n + 32, dtype=dt)
+        isz = np.dtype(dt).itemsize
+        base = (-buf.ctypes.data // isz) % (64 // isz)
+        view = buf[base + mis:base + mis + n]
+        st = getattr(lib, "rocrand_" + suffix)(g, ctypes.c_void_p(view.ctypes.data), ctypes.c_size_t(n),
+                                               *pyorc.dist_args(d, p))
+        assert st == ost == 0, (rng, d, st, ost)
+        assert np.array_equal(view, ovals), (rng, d)
+    lib.rocrand_destroy_generator(g)
+print("cpu-only ok")
+"""
+
+
+def test_cpu_only_process_without_env():
+    """A process that sees no CUDA device (CUDA_VISIBLE_DEVICES empty, no host-CPU switch)
+    gets host generators computed on the CPU, equal to the oracle."""
+    import subprocess
+    import sys
+    env = dict(os.environ)
+    env.pop("ROCRAND_B200_HOST_CPU", None)
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", CPU_ONLY_SCRIPT], cwd=root, env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "cpu-only ok" in r.stdout
