@@ -1,7 +1,7 @@
 """Host generators computed on the CPU (no GPU needed), against the oracle.
 
-In a process without a CUDA device -- or with ROCRAND_B200_HOST_CPU=1, set here so that the
-same test also runs the CPU form on a machine with a GPU -- rocrand_create_generator_host
+In a process without a CUDA device -- or with ROCRAND_B200_HOST_CPU=1, set here around each
+test so that it also runs the CPU form on a machine with a GPU -- rocrand_create_generator_host
 returns the generator in host execution: every generate call writes host memory through the
 same engine, output-order and distribution code as the kernels, compiled for the host, with
 the C library's fp32 transcendentals (the reference's host path takes the same ones).  Each
@@ -20,7 +20,13 @@ import pytest
 from oracle import pyorc
 from tests import gpu_util as gu
 
-os.environ["ROCRAND_B200_HOST_CPU"] = "1"
+
+
+@pytest.fixture(autouse=True)
+def _host_cpu(monkeypatch):
+    """Host execution for the generators these tests create (read at creation), and only
+    for them: the variable is removed again after each test."""
+    monkeypatch.setenv("ROCRAND_B200_HOST_CPU", "1")
 
 CPU_FAMILIES = {"xorwow": 401, "mrg32k3a": 402, "mtgp32": 403, "philox": 404, "mrg31k3p": 405,
                 "lfsr113": 406, "mt19937": 407, "threefry2x32": 408, "threefry2x64": 409,
