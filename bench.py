@@ -873,8 +873,9 @@ def serving_leg(lib, full):
     XORWOW, MRG32k3a, Sobol32; states resident), sizes log-uniform in [2^8, 2^26], dtypes
     uniform over fp32 / fp64 / uint32, a 64 GB output budget; the continuous-batching server
     and the plain per-request server replay the same trace.  Also a saturated trace (every
-    request at t=0).  Requests per trace: 10^5 at 50k req/s, 2000 otherwise (10^5 at every
-    rate with --full-configs).  For the saturated trace the report includes the bound of the
+    request at t=0).  Requests per trace: 10^5 at 50k req/s, 2000 for the saturated trace,
+    max(10^4, one second of arrivals) otherwise, so that each p99 rests on 100 or more
+    requests (10^5 at every rate with --full-configs).  For the saturated trace the report includes the bound of the
     batched/plain ratio that the mix allows: sum over requests of max(launch floor, device
     time) / sum of device times (serving_rates)."""
     import numpy as np
@@ -900,7 +901,7 @@ def serving_leg(lib, full):
                 htype.append(t)
         for rate in rates:
             rs = np.random.Generator(np.random.PCG64(7))
-            n = 100000 if (full or rate == 50000) else (2000 if (rate is None or rate >= 5000) else 1000)
+            n = 100000 if (full or rate == 50000) else (2000 if rate is None else max(10000, rate))
             gaps = rs.exponential(1.0 / rate, n) if rate else np.zeros(n)
             arrivals = np.cumsum(gaps) if rate else gaps
             hidx = rs.integers(0, len(handles), n)
@@ -944,9 +945,6 @@ def _ref_lib():
     if os.path.exists(pyorc.REF_PATH):
         return pyorc.CLib("ref"), "reference"
     return pyorc.CLib("orc"), "port"
-
-
-_SEEDED = {}  # MT19937 / MTGP32 host streams, seeded once per process
 
 
 _SEEDED = {}  # host generators per (call, threads, size): created, seeded and warmed once

@@ -611,6 +611,30 @@ struct FnMrgPoissonHuge
     }
 };
 
+// Transforms long enough (Box-Muller: a logarithm, a square root and a sine/cosine per
+// pair) that a thread gains from running two units side by side: MTGP32's fill takes two
+// units per step of its main loop for these.
+template<class F>
+struct long_transform : std::false_type
+{
+};
+template<>
+struct long_transform<FnNormalF> : std::true_type
+{
+};
+template<>
+struct long_transform<FnLogNormalF> : std::true_type
+{
+};
+template<>
+struct long_transform<FnNormalD> : std::true_type
+{
+};
+template<>
+struct long_transform<FnLogNormalD> : std::true_type
+{
+};
+
 template<class F>
 struct has_table
 {

@@ -321,6 +321,12 @@ constexpr bool kMtStaged = std::is_same<F, FnNormalD>::value || std::is_same<F, 
                            || std::is_same<F, FnNormalF>::value || std::is_same<F, FnLogNormalF>::value
                            || std::is_same<F, FnNormalH>::value || std::is_same<F, FnLogNormalH>::value;
 
+// Units a lane transforms side by side in a staged round inside the call: three fp64
+// Box-Muller chains, two fp32 / half ones.
+template<class F>
+constexpr unsigned kMtUnitsPerStep
+    = (std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value) ? 3u : 2u;
+
 // Shared memory of one block of mt_fill: the distribution's table, or the staged state.
 template<class F>
 inline size_t mt_fill_smem(const F& f)
@@ -381,9 +387,24 @@ __device__ __forceinline__ void round_edge(const U& u, const MtArgs& a, long lon
         ...);
 }
 
+// One input unit of a staged round: tempered slots G*iw .. G*iw+iw-1 through F.
+template<class F>
+__device__ __forceinline__ void staged_unit(const F& f, const uint32_t* s, unsigned G,
+                                            typename F::T (&out)[F::ow])
+{
+    uint32_t in[F::iw];
+#pragma unroll
+    for(unsigned i = 0; i < F::iw; i++)
+        in[i] = mt_temper(s[(G * F::iw + i) * kMtBlock]);
+    f(in, out);
+}
+
 // A round whose slots were staged in shared memory (slot j of this thread at s[j * 64]):
-// the slot groups are a loop, not an unrolled sequence, so one copy of the transform (two,
-// for two independent pairs in flight) stays in the instruction cache.
+// the slot groups are a loop, not an unrolled sequence, so the transform's code stays in the
+// instruction cache.  A round inside the call takes kMtUnitsPerStep units per iteration with
+// no branch between them, so their transform chains interleave (14 warps per SM hold every
+// MT lane: the latency is hidden by the lane's own independent work); the call's first and
+// last rounds take one unit at a time and skip the units outside the call.
 template<class F>
 __device__ __forceinline__ void mt_round_staged(const F& f, const uint32_t* s, const MtArgs& a, uint32_t rho)
 {
@@ -394,20 +415,39 @@ __device__ __forceinline__ void mt_round_staged(const F& f, const uint32_t* s, c
     const unsigned     tid = blockIdx.x * kMtBlock + threadIdx.x;
     const long long    base = static_cast<long long>(rho) * a.full - a.start;
     const long long    q0   = base + tid;
-    const bool interior = base >= 0 && static_cast<unsigned long long>(base) + a.full <= a.total;
-#pragma unroll 2
+    if(base >= 0 && static_cast<unsigned long long>(base) + a.full <= a.total)
+    {
+        constexpr unsigned U = kMtUnitsPerStep<F>;
+        unsigned           G = 0;
+#pragma unroll 1
+        for(; G + U <= per; G += U)
+        {
+            T o[U][ow];
+#pragma unroll
+            for(unsigned u = 0; u < U; u++)
+                staged_unit(f, s, G + u, o[u]);
+#pragma unroll
+            for(unsigned u = 0; u < U; u++)
+                store_vec(a.vec + static_cast<unsigned long long>(q0 + (G + u) * kMtThreads) * VB, o[u]);
+        }
+#pragma unroll 1
+        for(; G < per; G++)
+        {
+            T o0[ow];
+            staged_unit(f, s, G, o0);
+            store_vec(a.vec + static_cast<unsigned long long>(q0 + G * kMtThreads) * VB, o0);
+        }
+        return;
+    }
+#pragma unroll 1
     for(unsigned G = 0; G < per; G++)
     {
         const long long q = q0 + static_cast<long long>(G) * kMtThreads;
-        if(!interior && (q < 0 || static_cast<unsigned long long>(q) >= a.total))
+        if(q < 0 || static_cast<unsigned long long>(q) >= a.total)
             continue;
-        uint32_t in[F::iw];
-#pragma unroll
-        for(unsigned i = 0; i < F::iw; i++)
-            in[i] = mt_temper(s[(G * F::iw + i) * kMtBlock]);
         T out[ow];
-        f(in, out);
-        if(interior || static_cast<unsigned long long>(q) < a.vec_n)
+        staged_unit(f, s, G, out);
+        if(static_cast<unsigned long long>(q) < a.vec_n)
         {
             store_vec(a.vec + static_cast<unsigned long long>(q) * VB, out);
             continue;

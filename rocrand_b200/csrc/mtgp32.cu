@@ -27,6 +27,7 @@
 
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 extern "C" const unsigned char rb200_mtgp32_params_begin[];
@@ -55,8 +56,10 @@ struct MtgpArgs
     uint32_t           head, tail;
 };
 
+// 4 blocks of 256 threads per SM (at most 64 registers): all 512 block generators resident
+// at once on 148 SMs.
 template<class F>
-__global__ void __launch_bounds__(kMtgpBlock) mtgp_fill(MtgpArgs a, F fw)
+__global__ void __launch_bounds__(kMtgpBlock, 4) mtgp_fill(MtgpArgs a, F fw)
 {
     __shared__ uint32_t        s[kMtgpState];
     __shared__ uint32_t        tbl[16], tmp[16];
@@ -107,6 +110,27 @@ __global__ void __launch_bounds__(kMtgpBlock) mtgp_fill(MtgpArgs a, F fw)
     };
     // index < vec_n_down and index < vec_n_up are the same in the whole block (both are
     // multiples of 256), so every thread takes every step
+    if constexpr(long_transform<F>::value)
+    {
+        // two rounds' steps, then both transforms with no branch between them: the two
+        // Box-Muller chains interleave instead of each waiting out its own latency
+        while(index + str < a.vec_n_down)
+        {
+            uint32_t in0[F::iw], in1[F::iw];
+#pragma unroll
+            for(unsigned i = 0; i < F::iw; i++)
+                in0[i] = step();
+#pragma unroll
+            for(unsigned i = 0; i < F::iw; i++)
+                in1[i] = step();
+            T o0[ow], o1[ow];
+            f(in0, o0);
+            f(in1, o1);
+            store_small(a.vec + index * VB, o0);
+            store_small(a.vec + (index + str) * VB, o1);
+            index += 2 * str;
+        }
+    }
     while(index < a.vec_n_down)
     {
         gen();

@@ -396,10 +396,12 @@ private:
                 return;
             // What to start:
             //  * plain mode: one ordinary call per request on stream 0, queued back to back;
-            //  * otherwise, with two or more requests queued and a batch stream free: a batch
-            //    of what admission takes; with one queued (or every batch stream busy): that
-            //    request alone as an ordinary call on the single-request stream, so a lone
-            //    request waits neither for others to gather nor for a batch stream.
+            //  * otherwise, with kMinBatchQueue or more requests queued and a batch stream
+            //    free: a batch of what admission takes; with fewer queued (or every batch
+            //    stream busy): the oldest request alone as an ordinary call on the
+            //    single-request stream, so a short queue is served exactly as plain calls
+            //    (a batch's plan upload costs more than it saves for two or three small
+            //    requests) and no request waits for others to gather or for a batch stream.
             //  In both, admitted requests of at least kDirectBytes run as ordinary calls on
             //  the direct stream.
             int  s     = -1;
@@ -414,7 +416,7 @@ private:
                         s = static_cast<int>(k);
                         break;
                     }
-                batch = s >= 0 && m_queue.size() >= 2;
+                batch = s >= 0 && m_queue.size() >= kMinBatchQueue;
             }
             const bool single = !m_plain && !batch && m_singles < kPlainInFlight;
             if(!m_queue.empty() && (m_plain ? s >= 0 : (batch || single)))
@@ -517,6 +519,7 @@ private:
     }
 
     static constexpr size_t       kMaxBatchRequests = 8192;
+    static constexpr size_t       kMinBatchQueue    = 4;
     static constexpr size_t       kPlainInFlight  = 4096;
     static constexpr size_t       kDirectBytes    = size_t(32) << 20;
     static constexpr int          kDirectStream   = -1; // InFlight::stream of a direct call

@@ -144,31 +144,30 @@ bool logf_replay_device(lr::Table& out)
     std::lock_guard<std::mutex> lock(mu);
     if(!done[dev])
     {
-        // header: magic, bucket shift, bucket count, log2 slots, longest probe, stored, reachable
+        // header: magic, bucket shift, bucket count, log2 key buckets, members, reachable, 0
         const unsigned char* blob  = rb200_logf_replay_begin;
         const size_t         bytes = static_cast<size_t>(rb200_logf_replay_end - rb200_logf_replay_begin);
         uint32_t             h[6];
-        if(bytes < 32 || std::memcmp(blob, "RBLOGF01", 8) != 0)
+        if(bytes < 32 || std::memcmp(blob, "RBLOGF02", 8) != 0)
             return false;
         std::memcpy(h, blob + 8, sizeof(h));
-        const size_t bound_bytes = static_cast<size_t>(h[1]) * 2;
+        const size_t bound_bytes = static_cast<size_t>(h[1]) * 4;
         const size_t bound_pad   = (bound_bytes + 32 + 15) / 16 * 16 - 32;
-        const size_t slot_bytes  = (static_cast<size_t>(2) << h[2]) * 4;
-        if(h[0] != static_cast<uint32_t>(lr::kBucketShift) || h[1] != lr::kBuckets || h[2] < 1 || h[2] > 30
-           || bytes != 32 + bound_pad + slot_bytes)
+        const size_t key_bytes   = (static_cast<size_t>(4) << h[2]) * 4;
+        if(h[0] != static_cast<uint32_t>(lr::kBucketShift) || h[1] != lr::kBuckets || h[2] < 1 || h[2] > 28
+           || bytes != 32 + bound_pad + key_bytes)
             return false;
         void* d = nullptr;
-        if(cudaMalloc(&d, bound_pad + slot_bytes) != cudaSuccess)
+        if(cudaMalloc(&d, bound_pad + key_bytes) != cudaSuccess)
             return false;
-        if(cudaMemcpy(d, blob + 32, bound_pad + slot_bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        if(cudaMemcpy(d, blob + 32, bound_pad + key_bytes, cudaMemcpyHostToDevice) != cudaSuccess)
         {
             cudaFree(d);
             return false;
         }
-        cache[dev].bound      = static_cast<const uint16_t*>(d);
-        cache[dev].slots      = reinterpret_cast<const uint32_t*>(static_cast<const unsigned char*>(d) + bound_pad);
-        cache[dev].log2_slots = h[2];
-        cache[dev].max_probe  = h[3];
+        cache[dev].bound        = static_cast<const uint32_t*>(d);
+        cache[dev].keys         = reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(d) + bound_pad);
+        cache[dev].log2_buckets = h[2];
         done[dev]             = true;
     }
     out = cache[dev];

@@ -8,18 +8,23 @@
 //    uses its high word), p = 2^-32 + v 2^-32 rounded once (uniform_distribution,
 //    rocrand_uniform.h:61-64), x = 2p - 1, t = (1 - x)(1 + x), each operation rounded to
 //    float as the kernels round it.
-// 2. For each distinct t, the host's logf(t) against the kernels' own rounding f of the
-//    accurate logarithm (logf_replay.cuh base(), compiled here for the host: the same IEEE
-//    operations).  Where they differ, the argument and the host's result are stored, and
-//    the argument's bucket bound is raised to its distance from the rounding boundary.
-// 3. Every t is replayed through logf_replay.cuh logf_host() with the finished table and
+// 2. For each distinct t, the host's logf(t) against the kernels' float f of the logarithm
+//    (logf_replay.cuh base(), compiled here for the host: the same IEEE operations).  Where
+//    they differ, the host's result must be f's neighbour on the logarithm's side of f; the
+//    argument joins the member set, and the bound of its bucket and side is raised to its
+//    distance from the midpoint plus one.
+// 3. The member set goes into a bucketed two-choice hash table (four keys per bucket, cuckoo
+//    insertion; the table doubles until every key has a place).
+// 4. Every t is replayed through logf_replay.cuh logf_host() with the finished tables and
 //    must give the host's logf(t) bit for bit; otherwise nothing is written.
 //
-// Output (little-endian): "RBLOGF01", u32 bucket shift, u32 bucket count, u32 log2 of the
-// slot count, u32 longest probe, u32 stored arguments, u32 reachable arguments, u16 bounds
-// [bucket count] padded to 16 bytes, u32 slot pairs (argument bits, result bits)[slots].
+// Output (little-endian): "RBLOGF02", u32 bucket shift, u32 bucket count, u32 log2 of the
+// key-bucket count, u32 members, u32 reachable arguments, u32 0; u32 bounds [bucket count]
+// (side 0 in the low half, side 1 in the high half) padded to 16 bytes; u32 keys [4 x key
+// buckets].
 #include "logf_replay.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -35,6 +40,40 @@ float arg_of(uint32_t v)
     const float p = std::fmaf(static_cast<float>(v), 2.3283064e-10f, 2.3283064e-10f);
     const float x = 2.0f * p - 1.0f;
     return (1.0f - x) * (1.0f + x);
+}
+
+// Cuckoo insertion into 2^lb buckets of four; false when a key finds no place.
+bool build_keys(const std::vector<uint32_t>& members, uint32_t lb, std::vector<uint32_t>& keys)
+{
+    keys.assign(4ull << lb, 0u);
+    uint64_t rng = 0x243F6A8885A308D3ull;
+    for(uint32_t key : members)
+    {
+        uint32_t cur = key;
+        bool     placed = false;
+        for(int kick = 0; kick < 2000 && !placed; kick++)
+        {
+            const uint32_t h[2] = {lr::bucket1(cur, lb), lr::bucket2(cur, lb)};
+            for(int c = 0; c < 2 && !placed; c++)
+                for(int s = 0; s < 4 && !placed; s++)
+                    if(keys[4 * h[c] + s] == 0u)
+                    {
+                        keys[4 * h[c] + s] = cur;
+                        placed             = true;
+                    }
+            if(placed)
+                break;
+            // evict a random key of one of the two buckets; it moves to its other bucket
+            rng ^= rng << 13;
+            rng ^= rng >> 7;
+            rng ^= rng << 17;
+            const uint32_t slot = 4 * h[rng & 1] + static_cast<uint32_t>((rng >> 1) & 3);
+            std::swap(cur, keys[slot]);
+        }
+        if(!placed)
+            return false;
+    }
+    return true;
 }
 
 } // namespace
@@ -66,74 +105,68 @@ int main(int argc, char** argv)
 
     // 2. differences between the host's logf and the kernels' rounding
     const size_t          na = args.size();
-    std::vector<uint32_t> host(na);
-    std::vector<uint8_t>  differs(na, 0);
-    std::vector<uint32_t> dist(na, 0);
+    std::vector<uint32_t> host(na), dist(na, 0), side(na, 0);
+    std::vector<uint8_t>  state(na, 0); // 0 same, 1 member, 2 not in range, 3 not the neighbour
 #pragma omp parallel for schedule(dynamic, 4096)
     for(long long i = 0; i < static_cast<long long>(na); i++)
     {
         const float t = lr::ffrom(args[i]);
         host[i]       = lr::fbits(::logf(t));
-        if(!(t > 0.0f) || !(t <= 1.0f))
+        if(!(t >= 0x1p-64f) || !(t <= 1.0f))
         {
-            differs[i] = lr::fbits(pm::logf(t)) != host[i] ? 2 : 0; // must not happen
+            state[i] = lr::fbits(pm::logf(t)) != host[i] ? 2 : 0;
             continue;
         }
-        uint32_t    d;
-        const float f = lr::base(t, d);
+        uint32_t    d, s;
+        const float f = lr::base(t, d, s);
         dist[i]       = d;
-        differs[i]    = lr::fbits(f) != host[i] ? 1 : 0;
+        side[i]       = s;
+        if(lr::fbits(f) == host[i])
+            continue;
+        const uint32_t fb = lr::fbits(f);
+        const uint32_t nb = (s != 0u) == ((fb >> 31) == 0u) ? fb + 1u : fb - 1u;
+        state[i]          = nb == host[i] ? 1 : 3;
     }
-    std::vector<uint16_t> bound(lr::kBuckets, 0);
-    std::vector<size_t>   stored;
+    std::vector<uint32_t> bound(lr::kBuckets, 0);
+    std::vector<uint32_t> members;
     for(size_t i = 0; i < na; i++)
     {
-        if(differs[i] == 2)
+        if(state[i] >= 2)
         {
-            std::fprintf(stderr, "argument %08x outside (0, 1] differs from the host\n", args[i]);
+            std::fprintf(stderr, "argument %08x: %s\n", args[i],
+                         state[i] == 2 ? "outside [2^-64, 1] differs from the host"
+                                       : "the host's result is not the neighbour on the logarithm's side");
             return 1;
         }
-        if(differs[i] == 0)
+        if(state[i] == 0)
             continue;
         const uint32_t key = args[i] >> lr::kBucketShift;
-        const double   b   = static_cast<double>(dist[i]) + 1.0;
-        if(key >= lr::kBuckets || b > 65535.0)
+        const uint32_t b   = dist[i] + 1u;
+        if(key >= lr::kBuckets || b > 65535u)
         {
-            std::fprintf(stderr, "argument %08x: bucket %u, bound %.1f out of range\n", args[i], key, b);
+            std::fprintf(stderr, "argument %08x: bucket %u, bound %u out of range\n", args[i], key, b);
             return 1;
         }
-        bound[key] = std::max<uint16_t>(bound[key], static_cast<uint16_t>(b));
-        stored.push_back(i);
+        const uint32_t sh  = side[i] ? 16 : 0;
+        const uint32_t cur = (bound[key] >> sh) & 0xffffu;
+        if(b > cur)
+            bound[key] = (bound[key] & ~(0xffffu << sh)) | (b << sh);
+        members.push_back(args[i]);
     }
 
-    // open-addressing hash table at load <= 1/2
-    uint32_t log2s = 1;
-    while((1ull << log2s) < 2 * stored.size())
-        log2s++;
-    const uint32_t        mask = (1u << log2s) - 1u;
-    std::vector<uint32_t> slots(2ull << log2s, 0);
-    uint32_t              max_probe = 0;
-    for(size_t i : stored)
-    {
-        const uint32_t key = args[i];
-        uint32_t       h   = (key * lr::kHashMul) >> (32 - log2s);
-        uint32_t       k   = 1;
-        while(slots[2 * h] != 0)
-        {
-            h = (h + 1u) & mask;
-            k++;
-        }
-        slots[2 * h]     = key;
-        slots[2 * h + 1] = host[i];
-        max_probe        = std::max(max_probe, k);
-    }
+    // 3. the member set: key buckets at a load of at most 1/2
+    uint32_t lb = 1;
+    while((4ull << lb) < 2 * members.size())
+        lb++;
+    std::vector<uint32_t> keys;
+    while(!build_keys(members, lb, keys))
+        lb++;
 
-    // 3. replay every reachable argument through the kernels' code
+    // 4. replay every reachable argument through the kernels' code
     lr::Table tb;
-    tb.bound      = bound.data();
-    tb.slots      = slots.data();
-    tb.log2_slots = log2s;
-    tb.max_probe  = max_probe;
+    tb.bound        = bound.data();
+    tb.keys         = reinterpret_cast<const uint4*>(keys.data());
+    tb.log2_buckets = lb;
     long long bad = 0, probed = 0;
 #pragma omp parallel for schedule(dynamic, 4096) reduction(+ : bad, probed)
     for(long long i = 0; i < static_cast<long long>(na); i++)
@@ -141,30 +174,29 @@ int main(int argc, char** argv)
         const float t = lr::ffrom(args[i]);
         if(lr::fbits(lr::logf_host(t, tb)) != host[i])
             bad++;
-        if(t > 0.0f && t <= 1.0f)
+        if(t >= 0x1p-64f && t <= 1.0f)
         {
-            const uint16_t b = bound[args[i] >> lr::kBucketShift];
-            probed += (b != 0 && dist[i] <= b) ? 1 : 0;
+            const uint32_t b = (bound[args[i] >> lr::kBucketShift] >> (side[i] ? 16 : 0)) & 0xffffu;
+            probed += dist[i] < b ? 1 : 0;
         }
     }
     std::printf("logf replay: %zu reachable arguments, %zu differ from the kernels' rounding "
-                "(%.3f%%), %.2f%% looked up, %u slots, longest probe %u, %lld mismatches\n",
-                na, stored.size(), 100.0 * stored.size() / na, 100.0 * probed / na, mask + 1u,
-                max_probe, bad);
+                "(%.3f%%), %.2f%% looked up, %u key buckets, %lld mismatches\n",
+                na, members.size(), 100.0 * members.size() / na, 100.0 * probed / na, 1u << lb, bad);
     if(bad != 0)
         return 1;
 
     FILE* f = std::fopen(argv[1], "wb");
     if(!f)
         return 1;
-    const uint32_t hdr[6] = {static_cast<uint32_t>(lr::kBucketShift), lr::kBuckets, log2s, max_probe,
-                             static_cast<uint32_t>(stored.size()), static_cast<uint32_t>(na)};
-    std::fwrite("RBLOGF01", 1, 8, f);
+    const uint32_t hdr[6] = {static_cast<uint32_t>(lr::kBucketShift), lr::kBuckets, lb,
+                             static_cast<uint32_t>(members.size()), static_cast<uint32_t>(na), 0u};
+    std::fwrite("RBLOGF02", 1, 8, f);
     std::fwrite(hdr, 4, 6, f);
-    std::fwrite(bound.data(), 2, bound.size(), f);
-    const size_t pad = (16 - (8 + 24 + 2 * bound.size()) % 16) % 16;
+    std::fwrite(bound.data(), 4, bound.size(), f);
+    const size_t pad      = (16 - (8 + 24 + 4 * bound.size()) % 16) % 16;
     const char   zero[16] = {};
     std::fwrite(zero, 1, pad, f);
-    std::fwrite(slots.data(), 4, slots.size(), f);
+    std::fwrite(keys.data(), 4, keys.size(), f);
     return std::fclose(f) == 0 ? 0 : 1;
 }
