@@ -112,9 +112,9 @@ NCU_INST = {
     ("mt19937", "uniform"): 0.9146,
     ("mt19937", "uniform_double"): 1.3757,
     ("mt19937", "uniform_half"): 0.6749,
-    ("mt19937", "normal[0.0, 1.0]"): 2.3196,
-    ("mt19937", "normal_double[0.0, 1.0]"): 5.2681,
-    ("mt19937", "log_normal[0.0, 1.0]"): 2.6008,
+    ("mt19937", "normal[0.0, 1.0]"): 2.2395,
+    ("mt19937", "normal_double[0.0, 1.0]"): 5.0302,
+    ("mt19937", "log_normal[0.0, 1.0]"): 2.5208,
     ("mt19937", "poisson[0.5]"): 1.1601,
     ("mt19937", "poisson[10.0]"): 1.1608,
     ("mt19937", "poisson[1000.0]"): 1.1660,
@@ -128,13 +128,13 @@ NCU_INST = {
     ("threefry4x32_20", "poisson[0.5]"): 1.4929,
     ("threefry4x32_20", "poisson[10.0]"): 1.4938,
     ("threefry4x32_20", "poisson[1000.0]"): 1.5023,
-    ("mtgp32", "uint"): 1.1285,
-    ("mtgp32", "uniform"): 1.1989,
+    ("mtgp32", "uint"): 1.1253,
+    ("mtgp32", "uniform"): 1.1956,
     ("mtgp32", "uniform_double"): 2.9434,
     ("mtgp32", "uniform_half"): 0.8387,
-    ("mtgp32", "normal[0.0, 1.0]"): 2.9242,
-    ("mtgp32", "normal_double[0.0, 1.0]"): 5.9064,
-    ("mtgp32", "log_normal[0.0, 1.0]"): 3.2054,
+    ("mtgp32", "normal[0.0, 1.0]"): 2.4131,
+    ("mtgp32", "normal_double[0.0, 1.0]"): 5.9535,
+    ("mtgp32", "log_normal[0.0, 1.0]"): 2.6944,
     ("mtgp32", "poisson[0.5]"): 1.7156,
     ("mtgp32", "poisson[10.0]"): 1.7160,
     ("mtgp32", "poisson[1000.0]"): 1.7199,
@@ -806,6 +806,9 @@ def batched_leg(lib, full):
 
     plain_ms = timed(plain_pass, 2)
     plain_sum = checksum()
+    # the plain pass's bytes kept for a byte comparison when the device has room for a copy
+    free_bytes, _ = torch.cuda.mem_get_info()
+    keep = out.clone() if free_bytes > out.numel() + (4 << 30) else None
     out.zero_()
     rb.check_rocrand(lib.rocrand_b200_autotune_batch(c_void_p(stream.cuda_stream)))
     plan = c_void_p()
@@ -813,6 +816,9 @@ def batched_leg(lib, full):
                                                         c_void_p(stream.cuda_stream)))
     batch_ms = timed(lambda: lib.rocrand_b200_execute_batch_plan(plan, 1, c_void_p(stream.cuda_stream)), 5)
     batch_sum = checksum()
+    identical = bool(torch.equal(out, keep)) if keep is not None else plain_sum == batch_sum
+    compared  = "bytes" if keep is not None else "checksums"
+    del keep
     lib.rocrand_b200_destroy_batch_plan(plan)
     for g in gens:
         lib.rocrand_destroy_generator(g)
@@ -821,7 +827,8 @@ def batched_leg(lib, full):
             "batched_gbs": round(byte_count / (batch_ms * 1e-3) / 1e9, 1),
             "plain_gbs": round(byte_count / (plain_ms * 1e-3) / 1e9, 1),
             "speedup": round(plain_ms / batch_ms, 2), "batched_ms": round(batch_ms, 3),
-            "plain_ms": round(plain_ms, 3), "identical_outputs": plain_sum == batch_sum,
+            "plain_ms": round(plain_ms, 3), "identical_outputs": identical,
+            "compared": compared,
             "graph_replay": True, "autotuned": True,
             "sizes": "log-uniform [2^10, 2^24], PCG64 seed 42",
             "mix": "50% uniform fp32 / 30% normal fp32 / 20% Poisson 4"}

@@ -187,7 +187,7 @@ RB_PM_HD void sincos(double x, double& s_out, double& c_out)
     const double p2 = kd * RB_PIO2_2;
     double       rh, rl;
     two_sum(t, -p2, rh, rl);
-    rl -= kd * RB_PIO2_3;
+    rl = fma_(-kd, RB_PIO2_3, rl);
     {
         const double h = rh + rl;
         rl             = rl - (h - rh);
@@ -218,14 +218,14 @@ RB_PM_HD void sincos(double x, double& s_out, double& c_out)
     const double psl = fma_(ch, bh, -psh);
     double       ssh, ssl;
     fast_two_sum(sh, psh, ssh, ssl); // sin a >= sin(1/64) > |cos a * b| unless a = 0
-    const double s_low = ((ssl + psl) + sl) + ((sh * cm1 + ch * sinb_rest) + cl * bh);
+    const double s_low = ((ssl + psl) + sl) + fma_(cl, bh, fma_(sh, cm1, ch * sinb_rest));
     const double sv    = ssh + s_low;
     // cos(a + b) = cos a - (sin a * b) + cos a * (cos b - 1) - sin a * (sin b - b)
     const double pch = sh * bh;
     const double pcl = fma_(sh, bh, -pch);
     double       csh, csl;
     fast_two_sum(ch, -pch, csh, csl); // cos a >= 0.7 > |sin a * b|
-    const double c_low = ((csl - pcl) + cl) + ((ch * cm1 - sh * sinb_rest) - sl * bh);
+    const double c_low = ((csl - pcl) + cl) + fma_(-sl, bh, fma_(ch, cm1, -(sh * sinb_rest)));
     const double cv    = csh + c_low;
     const double s     = neg ? -sv : sv;
     // quadrant k: (sin, cos) = (s, c), (c, -s), (-s, -c), (-c, s)
