@@ -73,7 +73,7 @@ NCU_INST = {
     ("philox4x32_10", "uniform_double"): 0.8292,
     ("philox4x32_10", "uniform_half"): 0.2744,
     ("philox4x32_10", "normal[0.0, 1.0]"): 1.6415,
-    ("philox4x32_10", "normal_double[0.0, 1.0]"): 4.2726,
+    ("philox4x32_10", "normal_double[0.0, 1.0]"): 4.2097,
     ("philox4x32_10", "log_normal[0.0, 1.0]"): 1.9227,
     ("philox4x32_10", "poisson[0.5]"): 0.6473,
     ("philox4x32_10", "poisson[10.0]"): 0.6482,
@@ -83,7 +83,7 @@ NCU_INST = {
     ("xorwow", "uniform_double"): 0.6548,
     ("xorwow", "uniform_half"): 0.2766,
     ("xorwow", "normal[0.0, 1.0]"): 1.5476,
-    ("xorwow", "normal_double[0.0, 1.0]"): 4.0022,
+    ("xorwow", "normal_double[0.0, 1.0]"): 3.9299,
     ("xorwow", "log_normal[0.0, 1.0]"): 1.8289,
     ("xorwow", "poisson[0.5]"): 0.6151,
     ("xorwow", "poisson[10.0]"): 0.6155,
@@ -93,7 +93,7 @@ NCU_INST = {
     ("mrg32k3a", "uniform_double"): 1.2749,
     ("mrg32k3a", "uniform_half"): 0.7664,
     ("mrg32k3a", "normal[0.0, 1.0]"): 2.4937,
-    ("mrg32k3a", "normal_double[0.0, 1.0]"): 4.7173,
+    ("mrg32k3a", "normal_double[0.0, 1.0]"): 4.6392,
     ("mrg32k3a", "log_normal[0.0, 1.0]"): 2.7749,
     ("mrg32k3a", "poisson[0.5]"): 1.6234,
     ("mrg32k3a", "poisson[10.0]"): 1.6238,
@@ -103,7 +103,7 @@ NCU_INST = {
     ("lfsr113", "uniform_double"): 1.7893,
     ("lfsr113", "uniform_half"): 0.6060,
     ("lfsr113", "normal[0.0, 1.0]"): 2.0898,
-    ("lfsr113", "normal_double[0.0, 1.0]"): 5.0002,
+    ("lfsr113", "normal_double[0.0, 1.0]"): 4.9221,
     ("lfsr113", "log_normal[0.0, 1.0]"): 2.3711,
     ("lfsr113", "poisson[0.5]"): 1.2609,
     ("lfsr113", "poisson[10.0]"): 1.2613,
@@ -113,7 +113,7 @@ NCU_INST = {
     ("mt19937", "uniform_double"): 1.3757,
     ("mt19937", "uniform_half"): 0.6749,
     ("mt19937", "normal[0.0, 1.0]"): 2.2395,
-    ("mt19937", "normal_double[0.0, 1.0]"): 5.0302,
+    ("mt19937", "normal_double[0.0, 1.0]"): 4.9520,
     ("mt19937", "log_normal[0.0, 1.0]"): 2.5208,
     ("mt19937", "poisson[0.5]"): 1.1601,
     ("mt19937", "poisson[10.0]"): 1.1608,
@@ -123,7 +123,7 @@ NCU_INST = {
     ("threefry4x32_20", "uniform_double"): 2.5036,
     ("threefry4x32_20", "uniform_half"): 0.6872,
     ("threefry4x32_20", "normal[0.0, 1.0]"): 2.4985,
-    ("threefry4x32_20", "normal_double[0.0, 1.0]"): 5.8746,
+    ("threefry4x32_20", "normal_double[0.0, 1.0]"): 5.7965,
     ("threefry4x32_20", "log_normal[0.0, 1.0]"): 2.7797,
     ("threefry4x32_20", "poisson[0.5]"): 1.4929,
     ("threefry4x32_20", "poisson[10.0]"): 1.4938,
@@ -133,7 +133,7 @@ NCU_INST = {
     ("mtgp32", "uniform_double"): 2.9434,
     ("mtgp32", "uniform_half"): 0.8387,
     ("mtgp32", "normal[0.0, 1.0]"): 2.4131,
-    ("mtgp32", "normal_double[0.0, 1.0]"): 5.9535,
+    ("mtgp32", "normal_double[0.0, 1.0]"): 5.8832,
     ("mtgp32", "log_normal[0.0, 1.0]"): 2.6944,
     ("mtgp32", "poisson[0.5]"): 1.7156,
     ("mtgp32", "poisson[10.0]"): 1.7160,
@@ -143,7 +143,7 @@ NCU_INST = {
     ("mrg31k3p", "uniform_double"): 1.5029,
     ("mrg31k3p", "uniform_half"): 0.8962,
     ("mrg31k3p", "normal[0.0, 1.0]"): 2.6921,
-    ("mrg31k3p", "normal_double[0.0, 1.0]"): 4.8748,
+    ("mrg31k3p", "normal_double[0.0, 1.0]"): 4.7966,
     ("mrg31k3p", "log_normal[0.0, 1.0]"): 2.9734,
     ("mrg31k3p", "poisson[0.5]"): 1.8515,
     ("mrg31k3p", "poisson[10.0]"): 1.8518,
@@ -163,7 +163,7 @@ NCU_INST = {
     ("threefry2x64_20", "uniform_double"): 2.6899,
     ("threefry2x64_20", "uniform_half"): 0.7368,
     ("threefry2x64_20", "normal[0.0, 1.0]"): 2.6313,
-    ("threefry2x64_20", "normal_double[0.0, 1.0]"): 6.2311,
+    ("threefry2x64_20", "normal_double[0.0, 1.0]"): 6.1530,
     ("threefry2x64_20", "log_normal[0.0, 1.0]"): 2.9126,
     ("threefry2x64_20", "poisson[0.5]"): 2.9953,
     ("threefry2x64_20", "poisson[10.0]"): 2.9963,
@@ -173,7 +173,7 @@ NCU_INST = {
     ("threefry4x64_20", "uniform_double"): 2.6783,
     ("threefry4x64_20", "uniform_half"): 0.7388,
     ("threefry4x64_20", "normal[0.0, 1.0]"): 2.6241,
-    ("threefry4x64_20", "normal_double[0.0, 1.0]"): 6.1945,
+    ("threefry4x64_20", "normal_double[0.0, 1.0]"): 6.1164,
     ("threefry4x64_20", "log_normal[0.0, 1.0]"): 2.9053,
     ("threefry4x64_20", "poisson[0.5]"): 3.0316,
     ("threefry4x64_20", "poisson[10.0]"): 3.0327,

@@ -56,11 +56,6 @@ struct MtgpArgs
     uint32_t           head, tail;
 };
 
-// Transforms whose latency a thread hides by running two units side by side: the long
-// ones (Box-Muller) and the Poisson alias lookup (a shared-memory load on the step chain).
-template<class F>
-constexpr bool kMtgpPaired = long_transform<F>::value || std::is_same<F, FnPoisson>::value;
-
 // 4 blocks of 256 threads per SM (at most 64 registers): all 512 block generators resident
 // at once on 148 SMs.
 template<class F>
@@ -115,10 +110,10 @@ __global__ void __launch_bounds__(kMtgpBlock, 4) mtgp_fill(MtgpArgs a, F fw)
     };
     // index < vec_n_down and index < vec_n_up are the same in the whole block (both are
     // multiples of 256), so every thread takes every step
-    if constexpr(kMtgpPaired<F>)
+    if constexpr(long_transform<F>::value)
     {
         // two rounds' steps, then both transforms with no branch between them: the two
-        // transform chains interleave instead of each waiting out its own latency
+        // Box-Muller chains interleave instead of each waiting out its own latency
         while(index + str < a.vec_n_down)
         {
             uint32_t in0[F::iw], in1[F::iw];

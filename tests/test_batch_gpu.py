@@ -99,6 +99,24 @@ def test_batch_equals_plain_calls(lib, seed):
     _check(lib, reqs, _run_batch(lib, reqs))
 
 
+def test_batch_equals_oracle(lib, orc):
+    """Each request of a batch against the oracle directly, not only through the plain call
+    of the same generator: bit-exact classes identical, normals within the parity bound."""
+    _setup(lib)
+    reqs = _make(np.random.default_rng(77), 24)
+    got = _run_batch(lib, reqs)
+    for (t, d, seed, offset, n, mis), vals in zip(reqs, got):
+        name, params = DISTS[d]
+        calls = [(name, n, list(params), mis)]
+        s = None if t == rb.ROCRAND_RNG_QUASI_SOBOL32 else seed
+        (ost, ovals), = pyorc.run_sequence(orc, t, s, offset, calls)
+        assert ost == 0
+        if gu.bit_exact(t, name):
+            assert np.array_equal(vals.view(np.uint8), ovals.view(np.uint8)), (t, d, seed, offset, n, mis)
+        else:
+            gu.compare_call(orc, t, s, offset, None, calls, 0, vals, ovals)
+
+
 @pytest.mark.parametrize("use_graph", [0, 1])
 def test_batch_plan_and_graph_replay(lib, use_graph):
     _setup(lib)
