@@ -56,7 +56,8 @@ TWO_WORD = {"uniform_double", "normal", "normal_double", "log_normal", "log_norm
 # written once (at the capture's size part of the output was still in L2 when the kernel
 # ended and was written back after it), so a launch of B output bytes moves read + B.
 NCU_TRAFFIC = {
-    ("mt19937", "normal_double"): (20.66e6, "profiles/mt_fill_normal_double_n2p24.md"),
+    ("mt19937", "normal_double"): (20.53e6, "profiles/mt_fill_normal_double_n2p24.md"),
+    ("mtgp32", "normal_double"): (2.26e6, "profiles/mtgp_fill_normal_double_n2p24.md"),
     ("philox4x32_10", "uniform"): (0.01e6, "profiles/philox_fill_fast_uniform_n2p26.md"),
     ("philox4x32_10", "normal_double"): (0.05e6, "profiles/philox_fill_fast_normal_double_n2p24.md"),
     ("mtgp32", "uint"): (2.2e6, "profiles/mtgp_fill_uint_n2p24.md"),

@@ -77,7 +77,7 @@ def _alone(lib, rng, seed, calls):
 
 
 @pytest.mark.parametrize("plain", [0, 1])
-def test_results_equal_alone_and_in_the_mix(lib, plain):
+def test_results_equal_alone_and_in_the_mix(lib, orc, plain):
     _setup(lib)
     rs = np.random.default_rng(123 + plain)
     server = ctypes.c_void_p()
@@ -115,6 +115,22 @@ def test_results_equal_alone_and_in_the_mix(lib, plain):
             want = _alone(lib, t, seed, [(d, n) for _, d, n in mine])
             for (tk, d, n), w in zip(mine, want):
                 assert np.array_equal(results[tk].view(np.uint8), w.view(np.uint8)), (t, d, n)
+        # one handle per generator type against the oracle itself, not only through the
+        # plain calls: bit-exact classes identical, normals within the parity bound
+        seen = set()
+        for h, t, seed in handles:
+            if t in seen:
+                continue
+            seen.add(t)
+            mine = [(tk, d, n) for tk, hh, d, n in submitted if hh == h]
+            calls = [(DISTS[d][0], n, list(DISTS[d][1]), 0) for _, d, n in mine]
+            s = None if t == rb.ROCRAND_RNG_QUASI_SOBOL32 else seed
+            for k, ((tk, d, n), (ost, ovals)) in enumerate(zip(mine, pyorc.run_sequence(orc, t, s, None, calls))):
+                assert ost == 0
+                if gu.bit_exact(t, DISTS[d][0]):
+                    assert np.array_equal(results[tk].view(np.uint8), ovals.view(np.uint8)), (t, d, n)
+                else:
+                    gu.compare_call(orc, t, s, None, None, calls, k, results[tk], ovals)
     finally:
         assert lib.rocrand_b200_server_destroy(server) == 0
 

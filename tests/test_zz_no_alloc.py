@@ -1,4 +1,4 @@
-"""The Poisson entry point that allocates nothing, against the generator path.
+"""The Poisson entry point that allocates nothing, against the generator path and the oracle.
 
 Callers that cannot call cudaMalloc (inside a graph capture or a driver callback, or with
 device memory fully pre-partitioned) use rocrand_b200_generate_poisson_noalloc, whose alias
@@ -90,6 +90,25 @@ def test_noalloc_large_lambda_and_unaligned_output(lib, mis):
         torch.cuda.synchronize()
         assert np.array_equal(view.cpu().numpy(), want[k]), "call %d" % k
         offset += n
+
+
+def test_noalloc_equals_oracle(lib, orc):
+    """The entry point against the oracle directly: a Philox4x32-10 stream at a seed and an
+    offset, table and no-table lambdas, an aligned and a misaligned output."""
+    import torch
+    from oracle import pyorc
+    noalloc = _entry(lib)
+    stream = torch.cuda.current_stream().cuda_stream
+    for seed, offset, n, lam, mis in ((0x1234, 0, 200001, 10.0, 0), (77, 12345, 99999, 1000.0, 3),
+                                      (5, 7, 50003, 4500.0, 1)):
+        (ost, ovals), = pyorc.run_sequence(orc, rb.ROCRAND_RNG_PSEUDO_PHILOX4_32_10, seed, offset,
+                                           [("poisson", n, [lam], mis)])
+        assert ost == 0
+        buf = torch.empty(n + 8, dtype=torch.int32, device="cuda")
+        view = buf[mis:mis + n]
+        assert noalloc(seed, offset, ctypes.c_void_p(view.data_ptr()), n, lam, ctypes.c_void_p(stream)) == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(view.cpu().numpy().view(np.uint32), ovals.view(np.uint32)), (seed, offset, lam)
 
 
 def test_noalloc_inside_graph_capture(lib):
