@@ -56,6 +56,12 @@ struct MtgpArgs
     uint32_t           head, tail;
 };
 
+// Units a thread transforms side by side in the main loop: three fp64 Box-Muller chains,
+// two fp32 ones.
+template<class F>
+constexpr unsigned kMtgpUnits
+    = (std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value) ? 3u : 2u;
+
 // 4 blocks of 256 threads per SM (at most 64 registers): all 512 block generators resident
 // at once on 148 SMs.
 template<class F>
@@ -112,23 +118,25 @@ __global__ void __launch_bounds__(kMtgpBlock, 4) mtgp_fill(MtgpArgs a, F fw)
     // multiples of 256), so every thread takes every step
     if constexpr(long_transform<F>::value)
     {
-        // two rounds' steps, then both transforms with no branch between them: the two
+        // U rounds' steps, then their transforms with no branch between them: the U
         // Box-Muller chains interleave instead of each waiting out its own latency
-        while(index + str < a.vec_n_down)
+        constexpr unsigned U = kMtgpUnits<F>;
+        while(index + (U - 1) * str < a.vec_n_down)
         {
-            uint32_t in0[F::iw], in1[F::iw];
+            uint32_t in[U][F::iw];
 #pragma unroll
-            for(unsigned i = 0; i < F::iw; i++)
-                in0[i] = step();
+            for(unsigned u = 0; u < U; u++)
 #pragma unroll
-            for(unsigned i = 0; i < F::iw; i++)
-                in1[i] = step();
-            T o0[ow], o1[ow];
-            f(in0, o0);
-            f(in1, o1);
-            store_small(a.vec + index * VB, o0);
-            store_small(a.vec + (index + str) * VB, o1);
-            index += 2 * str;
+                for(unsigned i = 0; i < F::iw; i++)
+                    in[u][i] = step();
+            T o[U][ow];
+#pragma unroll
+            for(unsigned u = 0; u < U; u++)
+                f(in[u], o[u]);
+#pragma unroll
+            for(unsigned u = 0; u < U; u++)
+                store_small(a.vec + (index + u * str) * VB, o[u]);
+            index += U * str;
         }
     }
     while(index < a.vec_n_down)
