@@ -160,3 +160,38 @@ def test_cpu_only_process_without_env():
                        text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "cpu-only ok" in r.stdout
+
+
+OUTPUT = {"uint": 0, "uniform_double": 5, "normal": 7, "poisson": 13}
+POSITIONED = {"xorwow": 401, "mrg32k3a": 402, "mrg31k3p": 405, "lfsr113": 406, "philox": 404,
+              "threefry2x64": 409}
+
+
+@pytest.mark.parametrize("name", sorted(POSITIONED))
+@pytest.mark.parametrize("dist,params", [("uniform_double", []), ("normal", [0.0, 1.0]), ("uint", []),
+                                         ("poisson", [10.0])])
+def test_cpu_output_position_slices(lib, orc, name, dist, params):
+    """rocrand_b200_set_output_position on the CPU form: a generator positioned at output
+    r*n writes outputs [r*n, (r+1)*n) of the oracle's one long call, and continues it."""
+    rng = POSITIONED[name]
+    seed = 0xACE + rng
+    n = 2 * 131072 + 6
+    ranks = 3
+    (ost, whole), = pyorc.run_sequence(orc, rng, seed, None, [(dist, ranks * n, params, 0)])
+    assert ost == 0
+    for r in range(ranks):
+        g = ctypes.c_void_p()
+        assert lib.rocrand_create_generator_host(ctypes.byref(g), rng) == 0
+        try:
+            assert lib.rocrand_set_seed(g, seed) == 0
+            assert lib.rocrand_b200_set_output_position(g, OUTPUT[dist], r * n) == 0
+            st, part = host_generate(lib, g, dist, n, params, 0)
+            assert st == 0
+            st, more = host_generate(lib, g, dist, 1000, params, 0)
+            assert st == 0
+        finally:
+            lib.rocrand_destroy_generator(g)
+        assert np.array_equal(part.view(np.uint8), whole[r * n:(r + 1) * n].view(np.uint8)), (name, dist, r)
+        if r < ranks - 1:
+            assert np.array_equal(more.view(np.uint8),
+                                  whole[(r + 1) * n:(r + 1) * n + 1000].view(np.uint8)), (name, dist, r)
