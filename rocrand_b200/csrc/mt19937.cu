@@ -632,59 +632,67 @@ inline void mt_init_host(const uint32_t* seed_state, uint32_t* states)
         2);
 }
 
-// mt_fill on the host: generator g runs its eight lanes' slot groups round by round, with
-// mt_fill's unit numbering, skipping and extra unit; generators are independent.
+// mt_fill on the host: chunks of consecutive generators run round by round with mt_fill's
+// unit numbering, skipping and extra unit; within a round, slot group G of the chunk's lanes
+// is one contiguous run of units (unit = round base + lane index + G * 65536), written in
+// order.  Chunks are independent.
 template<class F>
 void mt_fill_host(const MtArgs& a, const F& f, uint32_t* states)
 {
-    using T                = typename F::T;
-    constexpr unsigned iw  = F::iw;
-    constexpr unsigned ow  = F::ow;
-    constexpr unsigned per = kMtSlots / iw;
-    constexpr unsigned VB  = sizeof(T) * ow;
+    using T                    = typename F::T;
+    constexpr unsigned iw      = F::iw;
+    constexpr unsigned ow      = F::ow;
+    constexpr unsigned per     = kMtSlots / iw;
+    constexpr unsigned VB      = sizeof(T) * ow;
+    constexpr unsigned kGenRun = 64; // generators per chunk (512 lanes)
     host_parallel_for(
-        kMtGens,
-        [&](unsigned long long g0, unsigned long long g1) {
-            for(unsigned long long g = g0; g < g1; g++)
+        kMtGens / kGenRun,
+        [&](unsigned long long c0, unsigned long long c1) {
+            for(unsigned long long c = c0; c < c1; c++)
             {
-                uint32_t* s = states + g * kMtN;
+                const unsigned long long g0 = c * kGenRun;
                 for(uint32_t rho = 0; rho < a.rounds; rho++)
                 {
                     if(rho > 0 || a.twist_first)
-                        mt_twist_host(s);
+                        for(unsigned long long g = g0; g < g0 + kGenRun; g++)
+                            mt_twist_host(states + g * kMtN);
                     const long long base = static_cast<long long>(rho) * a.full - a.start;
-                    for(unsigned lane = 0; lane < 8; lane++)
+                    for(unsigned G = 0; G < per; G++)
                     {
-                        const long long tid = static_cast<long long>(g * 8 + lane);
-                        for(unsigned G = 0; G < per; G++)
+                        for(unsigned long long g = g0; g < g0 + kGenRun; g++)
                         {
-                            const long long q = base + tid + static_cast<long long>(G) * kMtThreads;
-                            if(q < 0 || static_cast<unsigned long long>(q) >= a.total)
-                                continue;
-                            uint32_t in[iw];
-                            for(unsigned i = 0; i < iw; i++)
-                                in[i] = mt_temper(s[slot_word(lane, G * iw + i)]);
-                            T out[ow];
-                            f(in, out);
-                            if(static_cast<unsigned long long>(q) < a.vec_n)
+                            const uint32_t* s = states + g * kMtN;
+                            for(unsigned lane = 0; lane < 8; lane++)
                             {
-                                std::memcpy(a.vec + static_cast<unsigned long long>(q) * VB, out, VB);
-                                continue;
-                            }
-                            T* data = reinterpret_cast<T*>(a.data);
-                            for(unsigned o = 0; o < ow; o++)
-                            {
-                                if(o < a.head)
-                                    data[o] = out[o];
-                                if(static_cast<int>(o) > static_cast<int>(ow) - static_cast<int>(a.tail) - 1)
-                                    data[a.n + (ow - a.tail - 1) - o] = out[o];
+                                const long long q = base + static_cast<long long>(g * 8 + lane)
+                                                    + static_cast<long long>(G) * kMtThreads;
+                                if(q < 0 || static_cast<unsigned long long>(q) >= a.total)
+                                    continue;
+                                uint32_t in[iw];
+                                for(unsigned i = 0; i < iw; i++)
+                                    in[i] = mt_temper(s[slot_word(lane, G * iw + i)]);
+                                T out[ow];
+                                f(in, out);
+                                if(static_cast<unsigned long long>(q) < a.vec_n)
+                                {
+                                    std::memcpy(a.vec + static_cast<unsigned long long>(q) * VB, out, VB);
+                                    continue;
+                                }
+                                T* data = reinterpret_cast<T*>(a.data);
+                                for(unsigned o = 0; o < ow; o++)
+                                {
+                                    if(o < a.head)
+                                        data[o] = out[o];
+                                    if(static_cast<int>(o) > static_cast<int>(ow) - static_cast<int>(a.tail) - 1)
+                                        data[a.n + (ow - a.tail - 1) - o] = out[o];
+                                }
                             }
                         }
                     }
                 }
             }
         },
-        64);
+        2);
 }
 
 class Mt19937Generator final : public PseudoGeneratorBase

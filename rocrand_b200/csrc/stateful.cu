@@ -230,53 +230,48 @@ __global__ void __launch_bounds__(kBlock) stateful_fill(FillArgs a, F f)
         a.arena[static_cast<size_t>(k) * kE + e] = eng.w[k];
 }
 
-// The same output contract on the host (host generators without a GPU): slot t runs
-// stateful_fill's body for its engine; slots are independent (distinct engines, distinct
-// output vectors, the head and tail written by one slot), so they spread over the host's
-// cores.
+// The same output contract on the host (host generators without a GPU).  Slots are
+// independent (distinct engines, distinct output vectors, the head and tail written by one
+// slot), so chunks of consecutive slots spread over the host's cores; a chunk keeps its
+// engines in a local array and runs round by round (vector j = round * E + slot), so each
+// round writes one contiguous run of the output instead of one value every E vectors.
 template<class E, class F>
-static void stateful_slot_host(const FillArgs& a, const F& f, uint32_t t)
+static void stateful_edges_host(const FillArgs& a, const F& f, E& eng)
 {
-    const bool loops = t < a.vec_n;
-    const bool edges = F::ow > 1 && (a.head > 0 || a.tail > 0) && (a.vec_n % kE) == t;
-    if(!loops && !edges)
-        return;
-    const uint32_t e = (t + a.start) & (kE - 1);
-    E              eng;
-    for(int k = 0; k < E::kWords; k++)
-        eng.w[k] = a.arena[static_cast<size_t>(k) * kE + e];
     using T = typename F::T;
-    constexpr unsigned VB = F::ow * sizeof(T);
-    uint32_t           in[F::iw];
-    T                  out[F::ow];
-    unsigned long long j = t;
-    for(; j < a.vec_n; j += kE)
+    T        out[F::ow];
+    uint32_t in[F::iw];
+    T*       data = reinterpret_cast<T*>(a.data);
+    if(a.head > 0)
     {
         for(unsigned i = 0; i < F::iw; i++)
             in[i] = eng.next();
         f(in, out);
-        store_small(a.vec + j * VB, out);
+        for(unsigned o = 0; o < a.head; o++)
+            data[o] = out[o];
     }
-    if(F::ow > 1 && j == a.vec_n)
+    if(a.tail > 0)
     {
-        T* data = reinterpret_cast<T*>(a.data);
-        if(a.head > 0)
-        {
-            for(unsigned i = 0; i < F::iw; i++)
-                in[i] = eng.next();
-            f(in, out);
-            for(unsigned o = 0; o < a.head; o++)
-                data[o] = out[o];
-        }
-        if(a.tail > 0)
-        {
-            for(unsigned i = 0; i < F::iw; i++)
-                in[i] = eng.next();
-            f(in, out);
-            for(unsigned o = 0; o < a.tail; o++)
-                data[a.n - a.tail + o] = out[o];
-        }
+        for(unsigned i = 0; i < F::iw; i++)
+            in[i] = eng.next();
+        f(in, out);
+        for(unsigned o = 0; o < a.tail; o++)
+            data[a.n - a.tail + o] = out[o];
     }
+}
+
+template<class E>
+static void load_engine_host(const FillArgs& a, uint32_t t, E& eng)
+{
+    const uint32_t e = (t + a.start) & (kE - 1);
+    for(int k = 0; k < E::kWords; k++)
+        eng.w[k] = a.arena[static_cast<size_t>(k) * kE + e];
+}
+
+template<class E>
+static void store_engine_host(const FillArgs& a, uint32_t t, const E& eng)
+{
+    const uint32_t e = (t + a.start) & (kE - 1);
     for(int k = 0; k < E::kWords; k++)
         a.arena[static_cast<size_t>(k) * kE + e] = eng.w[k];
 }
@@ -284,14 +279,51 @@ static void stateful_slot_host(const FillArgs& a, const F& f, uint32_t t)
 template<class E, class F>
 static void stateful_fill_host(const FillArgs& a, const F& f)
 {
-    // slots below min(vec_n, E) loop; the edge slot vec_n % E is among them unless vec_n < E
+    using T                  = typename F::T;
+    constexpr unsigned VB    = F::ow * sizeof(T);
+    constexpr uint32_t kRun  = 1024; // slots per chunk
+    const bool         edges = F::ow > 1 && (a.head > 0 || a.tail > 0);
+    const uint32_t     te    = static_cast<uint32_t>(a.vec_n % kE); // the slot that writes them
+    // slots below min(vec_n, E) loop; the edge slot is among them unless vec_n < E
     const unsigned long long active = std::min<unsigned long long>(a.vec_n, kE);
-    host_parallel_for(active, [&](unsigned long long t0, unsigned long long t1) {
-        for(unsigned long long t = t0; t < t1; t++)
-            stateful_slot_host<E>(a, f, static_cast<uint32_t>(t));
-    });
-    if(a.vec_n < kE)
-        stateful_slot_host<E>(a, f, static_cast<uint32_t>(a.vec_n));
+    const unsigned long long chunks = (active + kRun - 1) / kRun;
+    host_parallel_for(
+        chunks,
+        [&](unsigned long long c0, unsigned long long c1) {
+            std::vector<E> eng(kRun);
+            for(unsigned long long c = c0; c < c1; c++)
+            {
+                const uint32_t t0 = static_cast<uint32_t>(c * kRun);
+                const uint32_t t1 = static_cast<uint32_t>(std::min<unsigned long long>(active, t0 + kRun));
+                for(uint32_t t = t0; t < t1; t++)
+                    load_engine_host(a, t, eng[t - t0]);
+                for(unsigned long long base = 0; base + t0 < a.vec_n; base += kE)
+                {
+                    const uint32_t last = static_cast<uint32_t>(std::min<unsigned long long>(t1, a.vec_n - base));
+                    for(uint32_t t = t0; t < last; t++)
+                    {
+                        uint32_t in[F::iw];
+                        T        out[F::ow];
+                        for(unsigned i = 0; i < F::iw; i++)
+                            in[i] = eng[t - t0].next();
+                        f(in, out);
+                        store_small(a.vec + (base + t) * VB, out);
+                    }
+                }
+                if(edges && te >= t0 && te < t1)
+                    stateful_edges_host(a, f, eng[te - t0]);
+                for(uint32_t t = t0; t < t1; t++)
+                    store_engine_host(a, t, eng[t - t0]);
+            }
+        },
+        2);
+    if(edges && a.vec_n < kE)
+    {
+        E eng;
+        load_engine_host(a, te, eng);
+        stateful_edges_host(a, f, eng);
+        store_engine_host(a, te, eng);
+    }
 }
 
 // ---------------------------------------------------------------------------------------
