@@ -195,3 +195,10 @@ def test_cpu_output_position_slices(lib, orc, name, dist, params):
         if r < ranks - 1:
             assert np.array_equal(more.view(np.uint8),
                                   whole[(r + 1) * n:(r + 1) * n + 1000].view(np.uint8)), (name, dist, r)
+
+
+def test_cpu_mt19937_calls_across_rounds(lib, orc):
+    """MT19937 on the CPU with calls longer than a round (65536 lanes x 78 slots) and one that
+    starts mid-round and crosses the next twist, against the oracle."""
+    run_case(lib, orc, 407, 0x600D, None, [("uint", 5200001, [], 0), ("uniform", 5500000, [], 1),
+                                           ("normal", 1001, [0.0, 1.0], 3), ("uint", 77, [], 2)])
