@@ -36,9 +36,44 @@ struct SobolCall
     const W*           scramble; // scrambled table, read at flat index dim (nullptr: plain)
     unsigned char*     data;
     unsigned long long n;       // points per dimension
+    unsigned long long chunk;   // points per block: a multiple of PPT * kBlock
     uint32_t           offset;
     SobolParams        p;
 };
+
+// Points per block for `dims` dimensions of n points each, blocks taking whole groups of
+// `group` points, on a GPU holding `wave` resident blocks: among the block counts per
+// dimension that fill k = 1 .. 64 waves (floor(k wave / dims) and one more), the one whose
+// grid leaves the least of its last wave idle, the fewest blocks on ties.
+inline unsigned long long sobol_chunk(unsigned long long n, unsigned long long dims, unsigned long long group,
+                                      unsigned long long wave)
+{
+    if(wave == 0)
+        wave = 1;
+    const unsigned long long groups     = (n + group - 1) / group;
+    unsigned long long       best_chunk = groups * group;
+    unsigned long long       best_nb    = 1;
+    double                   best_use   = 0.0;
+    auto                     consider   = [&](unsigned long long b) {
+        b                              = b < 1 ? 1 : (b > groups ? groups : b);
+        const unsigned long long chunk = (groups + b - 1) / b * group;
+        const unsigned long long nb    = (n + chunk - 1) / chunk;
+        const unsigned long long waves = (nb * dims + wave - 1) / wave;
+        const double             use   = static_cast<double>(nb * dims) / static_cast<double>(waves * wave);
+        if(use > best_use + 1e-3 || (use > best_use - 1e-3 && nb < best_nb))
+        {
+            best_chunk = chunk;
+            best_nb    = nb;
+            best_use   = use > best_use ? use : best_use;
+        }
+    };
+    for(unsigned long long k = 1; k <= 64; k++)
+    {
+        consider(k * wave / dims);
+        consider(k * wave / dims + 1);
+    }
+    return best_chunk;
+}
 
 template<class W, SobolKind K>
 __global__ void __launch_bounds__(kBlock) sobol_fill(SobolCall<W> a)
@@ -66,11 +101,16 @@ __global__ void __launch_bounds__(kBlock) sobol_fill(SobolCall<W> a)
 
     const W            c      = a.scramble ? a.scramble[dim] : W(0);
     T*                 row    = reinterpret_cast<T*>(a.data) + static_cast<size_t>(dim) * a.n;
-    const unsigned long long stride = static_cast<unsigned long long>(PPT) * gridDim.x * kBlock;
-    unsigned long long p      = (static_cast<unsigned long long>(blockIdx.x) * kBlock + threadIdx.x) * PPT;
-    if(p >= a.n)
+    // block x covers points [x chunk, (x + 1) chunk) of its dimension, its threads leap-frog
+    // through them by the power-of-two stride PPT * kBlock
+    constexpr unsigned long long stride = static_cast<unsigned long long>(PPT) * kBlock;
+    constexpr uint32_t           lg     = PPT == 4 ? 10u : (PPT == 8 ? 11u : 12u); // log2(stride)
+    static_assert((1ull << lg) == stride, "stride is a power of two");
+    const unsigned long long begin = static_cast<unsigned long long>(blockIdx.x) * a.chunk;
+    const unsigned long long end   = a.n < begin + a.chunk ? a.n : begin + a.chunk;
+    unsigned long long       p     = begin + static_cast<unsigned long long>(threadIdx.x) * PPT;
+    if(p >= end)
         return;
-    const uint32_t     lg     = __ffsll(static_cast<long long>(stride)) - 1; // log2(stride)
     const bool         vec_ok = (reinterpret_cast<uintptr_t>(row) % (PPT * sizeof(T))) == 0;
 
     // The engine starts at the 32-bit sum offset + p (sobol.hpp:191-196) and then counts in
@@ -84,7 +124,7 @@ __global__ void __launch_bounds__(kBlock) sobol_fill(SobolCall<W> a)
             if((g >> b) & 1)
                 x ^= v[b];
     }
-    for(; p < a.n; p += stride)
+    for(; p < end; p += stride)
     {
         T out[PPT];
         W xx = x;
@@ -302,15 +342,24 @@ private:
         a.n        = N;
         a.offset   = m_current;
         a.p        = p;
-        // power-of-two blocks per dimension, about 16 resident blocks per SM in total
-        const unsigned long long want = (N + kBlock * PPT - 1) / (kBlock * PPT);
-        const unsigned long long cap  = std::max<unsigned long long>(
-            1, static_cast<unsigned long long>(device_info().sm_count) * 16 / m_dims);
-        unsigned long long bx = 1;
-        while(bx * 2 <= std::min(want, cap))
-            bx *= 2;
-        const size_t smem = K == SobolKind::POISSON ? p.size * sizeof(double) : 0;
-        sobol_fill<W, K><<<dim3(static_cast<unsigned>(bx), m_dims), kBlock, smem, m_stream>>>(a);
+        // blocks per dimension: whole groups of PPT * kBlock points each, as many as fill the
+        // GPU's resident blocks in nearly whole waves
+        const size_t             smem  = K == SobolKind::POISSON ? p.size * sizeof(double) : 0;
+        constexpr unsigned long long group = static_cast<unsigned long long>(PPT) * kBlock;
+        const void* const kernel = reinterpret_cast<const void*>(sobol_fill<W, K>);
+        if(m_chunk_kernel != kernel || m_chunk_n != N || m_chunk_smem != smem || m_chunk_dims != m_dims)
+        {
+            const unsigned long long wave
+                = static_cast<unsigned long long>(device_info().sm_count) * blocks_per_sm(kernel, smem);
+            m_chunk        = sobol_chunk(N, m_dims, group, wave);
+            m_chunk_kernel = kernel;
+            m_chunk_n      = N;
+            m_chunk_smem   = smem;
+            m_chunk_dims   = m_dims;
+        }
+        a.chunk                        = m_chunk;
+        const unsigned long long nb    = (N + a.chunk - 1) / a.chunk;
+        sobol_fill<W, K><<<dim3(static_cast<unsigned>(nb), m_dims), kBlock, smem, m_stream>>>(a);
         return launch_status();
     }
 
@@ -363,6 +412,13 @@ private:
     unsigned int       m_dims        = 1;
     bool               m_initialized = false;
     PoissonCache       m_poisson;
+    // the block size in points of the last launch shape (kernel, points per dimension,
+    // shared memory, dimensions), chosen once per shape
+    const void*        m_chunk_kernel = nullptr;
+    unsigned long long m_chunk_n      = 0;
+    size_t             m_chunk_smem   = 0;
+    unsigned int       m_chunk_dims   = 0;
+    unsigned long long m_chunk        = 0;
 };
 
 rocrand_generator_base_type* make_sobol(rocrand_rng_type t)
