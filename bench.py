@@ -134,7 +134,7 @@ NCU_INST = {
     ("mtgp32", "uniform_double"): 2.9434,
     ("mtgp32", "uniform_half"): 0.8387,
     ("mtgp32", "normal[0.0, 1.0]"): 2.4131,
-    ("mtgp32", "normal_double[0.0, 1.0]"): 5.8832,
+    ("mtgp32", "normal_double[0.0, 1.0]"): 5.5306,
     ("mtgp32", "log_normal[0.0, 1.0]"): 2.6944,
     ("mtgp32", "poisson[0.5]"): 1.7156,
     ("mtgp32", "poisson[10.0]"): 1.7160,
@@ -808,6 +808,7 @@ def batched_leg(lib, full):
     plain_ms = timed(plain_pass, 2)
     plain_sum = checksum()
     # the plain pass's bytes kept for a byte comparison when the device has room for a copy
+    torch.cuda.empty_cache()  # earlier legs' cached blocks back to the device first
     free_bytes, _ = torch.cuda.mem_get_info()
     keep = out.clone() if free_bytes > out.numel() + (4 << 30) else None
     out.zero_()
