@@ -150,33 +150,6 @@ RB_PM_HD double log(double x)
     return x0 > 0.0 ? (x0 == INFINITY ? x0 : y) : (x0 == 0.0 ? -INFINITY : NAN);
 }
 
-// Natural logarithm to about one double ulp, for x in (0, 1]: the reduction of log() with
-// the sum in plain double.  Its float rounding is the correctly rounded logf except within
-// ~2^-29 ulp of a rounding boundary, which is what the host-logf replay needs from its base
-// (logf_replay.cuh), at a third of log()'s fp64 operations.
-RB_PM_HD double log_unit(double x)
-{
-    const uint64_t ix   = bits_of(x);
-    const uint64_t tmp  = ix - RB_LOG_OFF;
-    const unsigned i    = static_cast<unsigned>(tmp >> 44) & 255u;
-    const int      k    = static_cast<int>(static_cast<int64_t>(tmp) >> 52);
-    const double   z    = from_bits(ix - (tmp & 0xfff0000000000000ull));
-    const double*  row  = log_table() + 3 * i;
-    const double   invc = tab(row), lch = tab(row + 1), lcl = tab(row + 2);
-    const double   kd   = static_cast<double>(k);
-    const double   r    = fma_(z, invc, -1.0); // exact
-    const double   t1   = fma_(kd, RB_LN2_HI, lch);
-    // log1p(r) = r + r^2 (-1/2 + r/3 - r^2/4 + r^3/5 - r^4/6 + r^5/7); r^8/8 < 2^-67
-    double p = 1.0 / 7.0;
-    p        = fma_(p, r, -1.0 / 6.0);
-    p        = fma_(p, r, 1.0 / 5.0);
-    p        = fma_(p, r, -1.0 / 4.0);
-    p        = fma_(p, r, 1.0 / 3.0);
-    p        = fma_(p, r, -0.5);
-    const double u = fma_(r * r, p, r);
-    return t1 + (u + fma_(kd, RB_LN2_LO, lcl));
-}
-
 // sin and cos of x for 0 <= x < 8 (the Box-Muller angles 0 .. 2 pi), near-correctly rounded.
 RB_PM_HD void sincos(double x, double& s_out, double& c_out)
 {
