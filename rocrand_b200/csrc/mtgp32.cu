@@ -56,11 +56,11 @@ struct MtgpArgs
     uint32_t           head, tail;
 };
 
-// Units a thread transforms side by side in the main loop: three fp64 Box-Muller chains,
+// Units a thread transforms side by side in the main loop: four fp64 Box-Muller chains,
 // two fp32 ones.
 template<class F>
 constexpr unsigned kMtgpUnits
-    = (std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value) ? 3u : 2u;
+    = (std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value) ? 4u : 2u;
 
 // 4 blocks of 256 threads per SM (at most 64 registers): all 512 block generators resident
 // at once on 148 SMs.
