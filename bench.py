@@ -134,7 +134,7 @@ NCU_INST = {
     ("mtgp32", "uniform_double"): 2.9434,
     ("mtgp32", "uniform_half"): 0.8387,
     ("mtgp32", "normal[0.0, 1.0]"): 2.4131,
-    ("mtgp32", "normal_double[0.0, 1.0]"): 5.5306,
+    ("mtgp32", "normal_double[0.0, 1.0]"): 5.4471,
     ("mtgp32", "log_normal[0.0, 1.0]"): 2.6944,
     ("mtgp32", "poisson[0.5]"): 1.7156,
     ("mtgp32", "poisson[10.0]"): 1.7160,

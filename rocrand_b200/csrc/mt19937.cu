@@ -321,11 +321,11 @@ constexpr bool kMtStaged = std::is_same<F, FnNormalD>::value || std::is_same<F, 
                            || std::is_same<F, FnNormalF>::value || std::is_same<F, FnLogNormalF>::value
                            || std::is_same<F, FnNormalH>::value || std::is_same<F, FnLogNormalH>::value;
 
-// Units a lane transforms side by side in a staged round inside the call: three fp64
-// Box-Muller chains, two fp32 / half ones.
+// Units a lane transforms side by side in a staged round inside the call: four fp64
+// Box-Muller chains, three fp32 / half ones.
 template<class F>
 constexpr unsigned kMtUnitsPerStep
-    = (std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value) ? 3u : 2u;
+    = (std::is_same<F, FnNormalD>::value || std::is_same<F, FnLogNormalD>::value) ? 4u : 3u;
 
 // Shared memory of one block of mt_fill: the distribution's table, or the staged state.
 template<class F>
