@@ -47,7 +47,7 @@ struct Lfsr113Engine // rocrand_lfsr113.h:146-160
 {
     static constexpr int kWords  = 4;
     static constexpr int kGf2    = 4;
-    static constexpr int kUnroll = 1;
+    static constexpr int kUnroll = 2; // fill iterations unrolled together: consecutive transforms overlap
     uint32_t             w[kWords];
     __host__ __device__ __forceinline__ uint32_t next()
     {
