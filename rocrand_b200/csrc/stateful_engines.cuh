@@ -47,7 +47,7 @@ struct Lfsr113Engine // rocrand_lfsr113.h:146-160
 {
     static constexpr int kWords  = 4;
     static constexpr int kGf2    = 4;
-    static constexpr int kUnroll = 2; // fill iterations unrolled together: consecutive transforms overlap
+    static constexpr int kUnroll = 4; // fill iterations unrolled together: consecutive transforms overlap
     uint32_t             w[kWords];
     __host__ __device__ __forceinline__ uint32_t next()
     {
@@ -67,7 +67,7 @@ struct Lfsr113Engine // rocrand_lfsr113.h:146-160
 struct Mrg32k3aEngine // rocrand_mrg32k3a.h:160-190: g1[0..2], g2[0..2]
 {
     static constexpr int      kWords  = 6;
-    static constexpr int      kUnroll = 3;
+    static constexpr int      kUnroll = 6; // two rotation periods of the three-word components
     static constexpr uint64_t kM1 = 4294967087ull, kM2 = 4294944443ull;
     uint32_t                  w[kWords];
     // t < 2 m: t mod m, with the comparison and subtraction on 32-bit words (t - m < 2^32)
@@ -104,7 +104,7 @@ struct Mrg32k3aEngine // rocrand_mrg32k3a.h:160-190: g1[0..2], g2[0..2]
 struct Mrg31k3pEngine // rocrand_mrg31k3p.h:155-185: x1[0..2], x2[0..2]
 {
     static constexpr int      kWords  = 6;
-    static constexpr int      kUnroll = 3;
+    static constexpr int      kUnroll = 6; // two rotation periods of the three-word components
     static constexpr uint32_t kM1 = 2147483647u, kM2 = 2147462579u;
     uint32_t                  w[kWords];
     __host__ __device__ __forceinline__ uint32_t next()
