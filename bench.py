@@ -89,33 +89,33 @@ NCU_INST = {
     ("xorwow", "poisson[0.5]"): 0.6151,
     ("xorwow", "poisson[10.0]"): 0.6155,
     ("xorwow", "poisson[1000.0]"): 0.6190,
-    ("mrg32k3a", "uint"): 1.3374,
-    ("mrg32k3a", "uniform"): 1.3062,
-    ("mrg32k3a", "uniform_double"): 1.2749,
-    ("mrg32k3a", "uniform_half"): 0.7664,
-    ("mrg32k3a", "normal[0.0, 1.0]"): 2.4937,
-    ("mrg32k3a", "normal_double[0.0, 1.0]"): 4.6392,
-    ("mrg32k3a", "log_normal[0.0, 1.0]"): 2.7749,
-    ("mrg32k3a", "poisson[0.5]"): 1.6234,
-    ("mrg32k3a", "poisson[10.0]"): 1.6238,
-    ("mrg32k3a", "poisson[1000.0]"): 1.6273,
-    ("lfsr113", "uint"): 0.9768,
-    ("lfsr113", "uniform"): 1.0706,
-    ("lfsr113", "uniform_double"): 1.7893,
-    ("lfsr113", "uniform_half"): 0.6060,
-    ("lfsr113", "normal[0.0, 1.0]"): 2.0898,
-    ("lfsr113", "normal_double[0.0, 1.0]"): 4.9221,
-    ("lfsr113", "log_normal[0.0, 1.0]"): 2.3711,
-    ("lfsr113", "poisson[0.5]"): 1.2609,
-    ("lfsr113", "poisson[10.0]"): 1.2613,
-    ("lfsr113", "poisson[1000.0]"): 1.2647,
+    ("mrg32k3a", "uint"): 1.2554,
+    ("mrg32k3a", "uniform"): 1.2395,
+    ("mrg32k3a", "uniform_double"): 1.2139,
+    ("mrg32k3a", "uniform_half"): 0.7507,
+    ("mrg32k3a", "normal[0.0, 1.0]"): 2.4856,
+    ("mrg32k3a", "normal_double[0.0, 1.0]"): 4.6174,
+    ("mrg32k3a", "log_normal[0.0, 1.0]"): 2.7668,
+    ("mrg32k3a", "poisson[0.5]"): 1.5675,
+    ("mrg32k3a", "poisson[10.0]"): 1.5679,
+    ("mrg32k3a", "poisson[1000.0]"): 1.5714,
+    ("lfsr113", "uint"): 0.7690,
+    ("lfsr113", "uniform"): 0.8394,
+    ("lfsr113", "uniform_double"): 1.5347,
+    ("lfsr113", "uniform_half"): 0.4895,
+    ("lfsr113", "normal[0.0, 1.0]"): 1.9692,
+    ("lfsr113", "normal_double[0.0, 1.0]"): 4.7683,
+    ("lfsr113", "log_normal[0.0, 1.0]"): 2.2505,
+    ("lfsr113", "poisson[0.5]"): 1.0531,
+    ("lfsr113", "poisson[10.0]"): 1.0535,
+    ("lfsr113", "poisson[1000.0]"): 1.0570,
     ("mt19937", "uint"): 0.8396,
     ("mt19937", "uniform"): 0.9146,
     ("mt19937", "uniform_double"): 1.3757,
     ("mt19937", "uniform_half"): 0.6749,
-    ("mt19937", "normal[0.0, 1.0]"): 2.2395,
-    ("mt19937", "normal_double[0.0, 1.0]"): 4.9520,
-    ("mt19937", "log_normal[0.0, 1.0]"): 2.5208,
+    ("mt19937", "normal[0.0, 1.0]"): 2.2219,
+    ("mt19937", "normal_double[0.0, 1.0]"): 4.9500,
+    ("mt19937", "log_normal[0.0, 1.0]"): 2.5032,
     ("mt19937", "poisson[0.5]"): 1.1601,
     ("mt19937", "poisson[10.0]"): 1.1608,
     ("mt19937", "poisson[1000.0]"): 1.1660,
@@ -139,16 +139,16 @@ NCU_INST = {
     ("mtgp32", "poisson[0.5]"): 1.7156,
     ("mtgp32", "poisson[10.0]"): 1.7160,
     ("mtgp32", "poisson[1000.0]"): 1.7199,
-    ("mrg31k3p", "uint"): 1.5664,
-    ("mrg31k3p", "uniform"): 1.5352,
-    ("mrg31k3p", "uniform_double"): 1.5029,
-    ("mrg31k3p", "uniform_half"): 0.8962,
-    ("mrg31k3p", "normal[0.0, 1.0]"): 2.6921,
-    ("mrg31k3p", "normal_double[0.0, 1.0]"): 4.7966,
-    ("mrg31k3p", "log_normal[0.0, 1.0]"): 2.9734,
-    ("mrg31k3p", "poisson[0.5]"): 1.8515,
-    ("mrg31k3p", "poisson[10.0]"): 1.8518,
-    ("mrg31k3p", "poisson[1000.0]"): 1.8553,
+    ("mrg31k3p", "uint"): 1.4998,
+    ("mrg31k3p", "uniform"): 1.4685,
+    ("mrg31k3p", "uniform_double"): 1.4363,
+    ("mrg31k3p", "uniform_half"): 0.8748,
+    ("mrg31k3p", "normal[0.0, 1.0]"): 2.6685,
+    ("mrg31k3p", "normal_double[0.0, 1.0]"): 4.8044,
+    ("mrg31k3p", "log_normal[0.0, 1.0]"): 2.9497,
+    ("mrg31k3p", "poisson[0.5]"): 1.7848,
+    ("mrg31k3p", "poisson[10.0]"): 1.7852,
+    ("mrg31k3p", "poisson[1000.0]"): 1.7887,
     ("threefry2x32_20", "uint"): 1.2033,
     ("threefry2x32_20", "uniform"): 1.2814,
     ("threefry2x32_20", "uniform_double"): 2.5471,
