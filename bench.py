@@ -537,12 +537,29 @@ def run_ours(args):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
-    # detail: every kernel (device ms, fraction of its governing bound, that bound), then the
-    # short summaries of the other legs last
-    line["per_kernel"] = {r["kernel"]: [round(mean_call[i], 4), round(r["frac"], 3), r["bound"]]
-                          for i, r in enumerate(roofs)}
+    # every kernel (device ms, fraction of its governing bound, that bound) and the full
+    # comparison with the reference's kernels go to a details file beside the bench; the line
+    # keeps their summaries, so that it stays short enough to be kept whole
+    per_kernel = {r["kernel"]: [round(mean_call[i], 4), round(r["frac"], 3), r["bound"]] for i, r in enumerate(roofs)}
+    details_path = os.path.join(HERE, "bench_details.json")
+    try:
+        with open(details_path, "w") as fh:
+            json.dump({"per_kernel": per_kernel, "reference_kernels": refk}, fh, indent=1)
+        line["details"] = os.path.basename(details_path)
+    except OSError:
+        line["details"] = None
+    fracs = sorted(v[1] for v in per_kernel.values())
+    slowest = sorted(per_kernel.items(), key=lambda kv: -kv[1][0])[:6]
+    line["per_kernel_summary"] = {
+        "kernels": len(per_kernel), "frac_min": fracs[0], "frac_median": fracs[len(fracs) // 2],
+        "bound_counts": {b: sum(1 for v in per_kernel.values() if v[2] == b) for b in ("hbm", "issue")},
+        "slowest_ms_frac_bound": {k: v for k, v in slowest}}
     if refk is not None:
-        line["reference_kernels"] = refk
+        line["reference_kernels"] = {k: v for k, v in refk.items()
+                                     if k not in ("per_kernel_ms_ours_ref_ratio", "ref_normals_outside_host_bound")}
+        outside = refk.get("ref_normals_outside_host_bound") or {}
+        if outside:
+            line["reference_kernels"]["ref_normals_outside_host_bound_max"] = max(outside.values())
     if quasi is not None:
         line["quasi"] = quasi
     if batched is not None:
